@@ -1,0 +1,381 @@
+// ref_shim.cpp -- extern "C" binding onto the reference's own C++ API.
+//
+// TEST INFRASTRUCTURE ONLY. Compiled by oracle/Makefile together with the
+// reference's source files where they lie (src/core/*.cpp, src/apps/
+// cable_hanging.cpp, and for the GPU variant src/gpu/gpu_solver.cu and
+// src/gpu/gpu_batch.cpp), into oracle/_ref/. Nothing from the reference is
+// copied into this repository; this file only calls its public API:
+//   crs::Rod, makeStraightRod, makeRodFromCenterline, clampEndExact
+//     (src/core/rod.h:102-167)
+//   crs::step / SolverParams / SolverContext (src/core/solver.h:15-67)
+//   crs::CollisionWorld, generateContacts, selfCollisionIndexGap
+//     (src/core/collision.h:83-121)
+//   crs::colorStretchConstraints / colorBendConstraints (src/core/coloring.h:41-42)
+//   crs::gpu::Batch (src/gpu/gpu_solver.h:66-145), when REF_WITH_GPU is set.
+// Rods cross the boundary as orc_rod views (oracle/rod_oracle.h) in double.
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "apps/cable_hanging.h"
+#include "core/coloring.h"
+#include "core/collision.h"
+#include "core/rod.h"
+#include "core/solver.h"
+#include "rod_oracle.h"
+#ifdef REF_WITH_GPU
+#include "gpu/gpu_solver.h"
+#endif
+
+using namespace crs;
+
+namespace {
+
+Vec3 v3(const double* a) { return Vec3(a[0], a[1], a[2]); }
+void put3(double* a, int i, Vec3 v) {
+    a[3 * i] = v.x;
+    a[3 * i + 1] = v.y;
+    a[3 * i + 2] = v.z;
+}
+void put4(double* a, int i, Quat q) {
+    a[4 * i] = q.w;
+    a[4 * i + 1] = q.x;
+    a[4 * i + 2] = q.y;
+    a[4 * i + 3] = q.z;
+}
+Vec3 get3(const double* a, int i) { return Vec3(a[3 * i], a[3 * i + 1], a[3 * i + 2]); }
+Quat get4(const double* a, int i) { return Quat(a[4 * i], a[4 * i + 1], a[4 * i + 2], a[4 * i + 3]); }
+
+struct RodHandle {
+    Rod rod;
+    SolverContext ctx;
+    Coloring sc, bc;
+};
+
+struct WorldHandle {
+    CollisionWorld world;
+};
+
+RodMaterial material(double E, double nu, double rho, double r) {
+    RodMaterial m;
+    m.youngs = E;
+    m.poisson = nu;
+    m.density = rho;
+    m.radius = r;
+    return m;
+}
+
+}  // namespace
+
+extern "C" {
+
+void* ref_rod_straight(int n, double L, double E, double nu, double rho, double r,
+                       const double* origin, const double* dir) {
+    auto* h = new RodHandle();
+    h->rod = makeStraightRod(n, L, material(E, nu, rho, r), v3(origin), v3(dir));
+    return h;
+}
+
+void* ref_rod_centerline(const double* pts, int numPoints, double E, double nu, double rho,
+                         double r, const double* seed, double twist) {
+    std::vector<Vec3> p(numPoints);
+    for (int i = 0; i < numPoints; ++i) p[i] = get3(pts, i);
+    auto* h = new RodHandle();
+    h->rod = makeRodFromCenterline(p, material(E, nu, rho, r), v3(seed), twist);
+    return h;
+}
+
+// The cable of src/apps/cable_hanging.cpp:18-47 (material of
+// cable_hanging.cpp:9-16: r = 4 mm, rho = 1100, nu = 0.35) at the given task
+// geometry, leg ratio and modulus.
+void* ref_rod_hanging(double length, int segments, double barRadius, double barHeight,
+                      double legRatio, double youngs) {
+    apps::HangingCable task;
+    task.length = length;
+    task.segments = segments;
+    task.barRadius = barRadius;
+    task.barHeight = barHeight;
+    auto* h = new RodHandle();
+    h->rod = task.build(legRatio, youngs);
+    return h;
+}
+
+void ref_rod_free(void* h) { delete static_cast<RodHandle*>(h); }
+
+int ref_rod_clamp(void* h, int tip) { return clampEndExact(static_cast<RodHandle*>(h)->rod, tip != 0); }
+
+void ref_rod_set_rest_from_current(void* h) { setRestFromCurrent(static_cast<RodHandle*>(h)->rod); }
+
+void ref_rod_sizes(void* h, int* out) {
+    const Rod& r = static_cast<RodHandle*>(h)->rod;
+    out[0] = int(r.state.numParticles());
+    out[1] = int(r.state.numSegments());
+    out[2] = int(r.stretch.size());
+    out[3] = int(r.bend.size());
+}
+
+// Copy every array of the reference Rod into caller-allocated orc_rod arrays.
+void ref_rod_export(void* hp, orc_rod* o) {
+    const Rod& r = static_cast<RodHandle*>(hp)->rod;
+    const RodState& s = r.state;
+    o->nP = int(s.numParticles());
+    o->nS = int(s.numSegments());
+    o->nSt = int(r.stretch.size());
+    o->nB = int(r.bend.size());
+    o->radius = r.material.radius;
+    o->youngs = r.material.youngs;
+    o->poisson = r.material.poisson;
+    o->density = r.material.density;
+    for (int i = 0; i < o->nP; ++i) {
+        put3(o->x, i, s.x[i]);
+        put3(o->xPrev, i, s.xPrev[i]);
+        put3(o->v, i, s.v[i]);
+        o->invMass[i] = s.invMass[i];
+        o->mass[i] = s.mass[i];
+        put3(o->extForce, i, s.extForce[i]);
+        put3(o->kinVel, i, s.kinematicVelocity[i]);
+    }
+    for (int j = 0; j < o->nS; ++j) {
+        put4(o->q, j, s.q[j]);
+        put4(o->qPrev, j, s.qPrev[j]);
+        put3(o->omega, j, s.omega[j]);
+        put3(o->invInertia, j, s.invInertia[j]);
+        put3(o->inertia, j, s.inertia[j]);
+        put3(o->extTorque, j, s.extTorque[j]);
+    }
+    for (int k = 0; k < o->nSt; ++k) {
+        o->sP0[k] = r.stretch.p0[k];
+        o->sP1[k] = r.stretch.p1[k];
+        o->sSeg[k] = r.stretch.seg[k];
+        o->sRest[k] = r.stretch.restLength[k];
+        put3(o->sComp, k, r.stretch.compliance[k]);
+        put3(o->sLam, k, r.stretch.lambda[k]);
+    }
+    for (int k = 0; k < o->nB; ++k) {
+        o->bA[k] = r.bend.segA[k];
+        o->bB[k] = r.bend.segB[k];
+        o->bRest[k] = r.bend.restLength[k];
+        put3(o->bRestD, k, r.bend.restDarboux[k]);
+        put3(o->bComp, k, r.bend.compliance[k]);
+        put3(o->bLam, k, r.bend.lambda[k]);
+    }
+}
+
+// Overwrite the reference Rod's state and loads from an orc_rod of the same
+// topology (positions, velocities, frames, loads; not topology or material).
+void ref_rod_import_state(void* hp, const orc_rod* o) {
+    Rod& r = static_cast<RodHandle*>(hp)->rod;
+    RodState& s = r.state;
+    for (int i = 0; i < o->nP; ++i) {
+        s.x[i] = get3(o->x, i);
+        s.xPrev[i] = get3(o->xPrev, i);
+        s.v[i] = get3(o->v, i);
+        s.extForce[i] = get3(o->extForce, i);
+        s.kinematicVelocity[i] = get3(o->kinVel, i);
+        s.invMass[i] = o->invMass[i];
+    }
+    for (int j = 0; j < o->nS; ++j) {
+        s.q[j] = get4(o->q, j);
+        s.qPrev[j] = get4(o->qPrev, j);
+        s.omega[j] = get3(o->omega, j);
+        s.extTorque[j] = get3(o->extTorque, j);
+    }
+    for (int k = 0; k < o->nB; ++k) r.bend.restDarboux[k] = get3(o->bRestD, k);
+}
+
+void* ref_world_create(const orc_prim* prims, int numPrims, int selfCollision, double selfFriction,
+                       int selfSkip, int hashTableSize, double marginRadii) {
+    auto* w = new WorldHandle();
+    for (int k = 0; k < numPrims; ++k) {
+        const orc_prim& p = prims[k];
+        Primitive q;
+        q.type = p.type;
+        q.a = v3(p.a);
+        q.b = v3(p.b);
+        q.normal = v3(p.normal);
+        q.halfExtents = v3(p.halfExtents);
+        q.rotation = Quat(p.rotation[0], p.rotation[1], p.rotation[2], p.rotation[3]);
+        q.radius = p.radius;
+        q.friction = p.friction;
+        w->world.primitives.push_back(q);
+    }
+    w->world.selfCollision = selfCollision != 0;
+    w->world.selfFriction = selfFriction;
+    w->world.selfSkip = selfSkip;
+    w->world.hashTableSize = hashTableSize;
+    w->world.contactMarginRadii = marginRadii;
+    return w;
+}
+
+void ref_world_free(void* w) { delete static_cast<WorldHandle*>(w); }
+
+int ref_self_gap(void* h, void* w) {
+    return selfCollisionIndexGap(static_cast<RodHandle*>(h)->rod, static_cast<WorldHandle*>(w)->world);
+}
+
+// Colourings: returns numColors; order has count entries, colorStart numColors+1.
+int ref_coloring(void* hp, int bend, int* order, int* colorStart) {
+    const Rod& r = static_cast<RodHandle*>(hp)->rod;
+    const Coloring c = bend ? colorBendConstraints(r) : colorStretchConstraints(r);
+    std::copy(c.order.begin(), c.order.end(), order);
+    std::copy(c.colorStart.begin(), c.colorStart.end(), colorStart);
+    return c.numColors();
+}
+
+static SolverParams params(double dt, int substeps, int iterations, const double* g, double lin,
+                           double ang, int interval) {
+    SolverParams p;
+    p.dt = dt;
+    p.substeps = substeps;
+    p.iterations = iterations;
+    p.gravity = v3(g);
+    p.linearDamping = lin;
+    p.angularDamping = ang;
+    p.contactInterval = interval;
+    return p;
+}
+
+// `colored` != 0 runs the sweep in the GPU's colour order (solver.h:31-36).
+void ref_step(void* hp, void* wp, double dt, int substeps, int iterations, const double* g,
+              double lin, double ang, int interval, int colored, int steps) {
+    auto* h = static_cast<RodHandle*>(hp);
+    SolverParams p = params(dt, substeps, iterations, g, lin, ang, interval);
+    if (colored) {
+        h->sc = colorStretchConstraints(h->rod);
+        h->bc = colorBendConstraints(h->rod);
+        p.stretchColoring = &h->sc;
+        p.bendColoring = &h->bc;
+    }
+    for (int s = 0; s < steps; ++s) {
+        if (wp)
+            step(h->rod, p, static_cast<WorldHandle*>(wp)->world, h->ctx);
+        else
+            step(h->rod, p);
+    }
+}
+
+// Many rods on `threads` host threads, contiguous rod ranges per thread
+// (src/validation/scaling_cases.cpp:431-438). Returns wall seconds.
+double ref_step_many(void** rods, void** worlds, int numRods, double dt, int substeps,
+                     int iterations, const double* g, double lin, double ang, int interval,
+                     int steps, int threads) {
+    SolverParams base = params(dt, substeps, iterations, g, lin, ang, interval);
+    for (int r = 0; r < numRods; ++r) {
+        auto* h = static_cast<RodHandle*>(rods[r]);
+        h->sc = colorStretchConstraints(h->rod);
+        h->bc = colorBendConstraints(h->rod);
+    }
+    auto work = [&](int b, int e) {
+        for (int r = b; r < e; ++r) {
+            auto* h = static_cast<RodHandle*>(rods[r]);
+            SolverParams p = base;
+            p.stretchColoring = &h->sc;
+            p.bendColoring = &h->bc;
+            for (int s = 0; s < steps; ++s) {
+                if (worlds && worlds[r])
+                    step(h->rod, p, static_cast<WorldHandle*>(worlds[r])->world, h->ctx);
+                else
+                    step(h->rod, p);
+            }
+        }
+    };
+    threads = std::max(1, std::min(threads, numRods));
+    const auto t0 = std::chrono::steady_clock::now();
+    std::vector<std::thread> pool;
+    const int per = (numRods + threads - 1) / threads;
+    for (int t = 0; t < threads; ++t) {
+        const int b = t * per, e = std::min(numRods, b + per);
+        if (b < e) pool.emplace_back(work, b, e);
+    }
+    for (auto& th : pool) th.join();
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// The rod's current contact list (the one the last substep used), as
+// idx[4], weight[4], normal[3], offset, friction, lambdaN per contact.
+int ref_contacts(void* hp, int* idx, double* weight, double* normal, double* offset, int cap) {
+    const ContactSet& cs = static_cast<RodHandle*>(hp)->ctx.contacts;
+    const int n = int(cs.contacts.size());
+    for (int c = 0; c < n && c < cap; ++c) {
+        const Contact& k = cs.contacts[c];
+        for (int m = 0; m < 4; ++m) {
+            idx[4 * c + m] = k.idx[m];
+            weight[4 * c + m] = k.weight[m];
+        }
+        put3(normal, c, k.normal);
+        offset[c] = k.offset;
+    }
+    return n;
+}
+
+// Fresh contact generation at the rod's current state (collision.cpp:76-152).
+int ref_generate_contacts(void* hp, void* wp, int* idx, double* weight, double* normal,
+                          double* offset, int cap) {
+    auto* h = static_cast<RodHandle*>(hp);
+    generateContacts(h->rod, static_cast<WorldHandle*>(wp)->world, h->ctx.contacts, h->ctx.hash);
+    return ref_contacts(hp, idx, weight, normal, offset, cap);
+}
+
+#ifdef REF_WITH_GPU
+// ---- the reference GPU batch (src/gpu/gpu_solver.h:66-145) ----
+void* refgpu_create(void* hp, int numRods, int fused, void* wp) {
+    auto* b = new gpu::Batch();
+    const CollisionWorld* w = wp ? &static_cast<WorldHandle*>(wp)->world : nullptr;
+    if (!b->create(static_cast<RodHandle*>(hp)->rod, numRods,
+                   fused ? gpu::Strategy::kFused : gpu::Strategy::kMultiKernel, w)) {
+        delete b;
+        return nullptr;
+    }
+    return b;
+}
+void refgpu_free(void* b) { delete static_cast<gpu::Batch*>(b); }
+void refgpu_step(void* b, double dt, int substeps, int iterations, const double* g, double lin,
+                 double ang, int interval, int steps) {
+    gpu::BatchParams p;
+    p.dt = float(dt);
+    p.substeps = substeps;
+    p.iterations = iterations;
+    p.gravityX = float(g[0]);
+    p.gravityY = float(g[1]);
+    p.gravityZ = float(g[2]);
+    p.linearDamping = float(lin);
+    p.angularDamping = float(ang);
+    p.contactInterval = interval;
+    for (int s = 0; s < steps; ++s) static_cast<gpu::Batch*>(b)->step(p);
+}
+void refgpu_sync(void* b) { static_cast<gpu::Batch*>(b)->synchronize(); }
+void refgpu_download(void* b, int rod, void* hp) {
+    static_cast<gpu::Batch*>(b)->download(rod, static_cast<RodHandle*>(hp)->rod);
+}
+void refgpu_upload_rod(void* b, int rod, void* hp) {
+    static_cast<gpu::Batch*>(b)->uploadRod(rod, static_cast<RodHandle*>(hp)->rod);
+}
+void refgpu_set_loads(void* b, int rod, void* hp) {
+    static_cast<gpu::Batch*>(b)->setLoads(rod, static_cast<RodHandle*>(hp)->rod);
+}
+void refgpu_set_kinematic(void* b, const float* xyz, long n) {
+    std::vector<Vec3f> v(n);
+    for (long i = 0; i < n; ++i) v[i] = Vec3f(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+    static_cast<gpu::Batch*>(b)->setKinematicVelocities(v);
+}
+void refgpu_set_material_scales(void* b, const float* youngs, const float* friction, int n) {
+    std::vector<float> y(youngs ? youngs : nullptr, youngs ? youngs + n : nullptr);
+    std::vector<float> f(friction ? friction : nullptr, friction ? friction + n : nullptr);
+    static_cast<gpu::Batch*>(b)->setMaterialScales(y, f);
+}
+void refgpu_download_positions(void* b, float* out) {
+    std::vector<Vec3f> v;
+    static_cast<gpu::Batch*>(b)->downloadPositions(v);
+    for (std::size_t i = 0; i < v.size(); ++i) {
+        out[3 * i] = v[i].x;
+        out[3 * i + 1] = v[i].y;
+        out[3 * i + 2] = v[i].z;
+    }
+}
+long long refgpu_overflow(void* b) { return static_cast<gpu::Batch*>(b)->selfContactOverflow(); }
+int refgpu_available() { return gpu::cudaAvailable() ? 1 : 0; }
+#endif
+
+}  // extern "C"
