@@ -1,0 +1,341 @@
+/*
+ * ropephysics_b200.h -- C ABI of the B200-native batched XPBD Cosserat-rod step.
+ *
+ * This is the drop-in boundary for RopePhysics' batched GPU rod step. Every
+ * entry point below replaces one reference interface, cited as file:line in
+ * the reference project:
+ *   crs::gpu::Batch and its free functions   src/gpu/gpu_solver.h:44-150
+ *   the rod descriptors and builders         src/core/rod.h:26-170
+ *   the collision world / primitives         src/core/collision.h:83-106,
+ *                                            src/core/geometry.h:17-65
+ *   constraint colouring                     src/core/coloring.h:22-51
+ *
+ * Conventions
+ *   - Plain C: POD structs, pointers and sizes; no C++ or CUDA types.
+ *   - Host data is double precision, exactly as the reference's Rod; the device
+ *     runs FP32 (with optional FP64 decision points, see rp_precision).
+ *   - Vectors are packed xyz, quaternions packed wxyz (body -> world).
+ *   - Every function returns rp_status; RP_OK is 0. On failure,
+ *     rp_last_error() returns a message for the calling thread.
+ *   - A handle is not thread-safe; use one host thread per rp_batch.
+ *   - rp_batch_step() is asynchronous on the batch's stream (the reference's
+ *     Batch::step is asynchronous on the default stream); download/read calls
+ *     synchronize that stream first.
+ */
+#ifndef ROPEPHYSICS_B200_H
+#define ROPEPHYSICS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RP_ABI_VERSION 1
+
+typedef enum rp_status {
+    RP_OK = 0,
+    RP_ERR_INVALID = 1,       /* malformed argument or descriptor */
+    RP_ERR_NO_DEVICE = 2,     /* no usable CUDA device (reference: create() false) */
+    RP_ERR_SHARED_MEMORY = 3, /* a rod does not fit the strategy's shared memory
+                                 (reference: gpu_batch.cpp:173-182) */
+    RP_ERR_OUT_OF_MEMORY = 4, /* device allocation failed (gpu_batch.cpp:275-311) */
+    RP_ERR_CUDA = 5,          /* a CUDA call or kernel launch failed */
+    RP_ERR_BUDGET = 6,        /* serving: request exceeds the HBM budget */
+    RP_ERR_NOT_READY = 7      /* serving: result not available yet */
+} rp_status;
+
+/* Execution strategy (reference: crs::gpu::Strategy, gpu_solver.h:50).
+ *   RP_STRATEGY_MULTI_KERNEL  accepted for source compatibility: one CTA per
+ *                             rod with all state in global memory, so any rod
+ *                             length runs. Results equal RP_STRATEGY_FUSED bit
+ *                             for bit (same kernel code, same order).
+ *   RP_STRATEGY_FUSED         the plain one-rod-per-CTA step: state resident
+ *                             in shared memory for the whole step (up to the
+ *                             227 KB opt-in on B200).
+ *   RP_STRATEGY_BATCHED       the persistent form: rods sorted by length into
+ *                             groups, several rods per CTA, warp-synchronous
+ *                             colour sweeps, work queue over all SMs. */
+typedef enum rp_strategy {
+    RP_STRATEGY_MULTI_KERNEL = 0,
+    RP_STRATEGY_FUSED = 1,
+    RP_STRATEGY_BATCHED = 2
+} rp_strategy;
+
+/* Precision flags (bitwise OR). 0 = reference order: every FP32 operation in
+ * the order of the reference kernel, for parity with its GPU path.
+ *   RP_PRECISION_COMPENSATED  Kahan-compensated position accumulation.
+ *   RP_PRECISION_FP64_CONE    the Coulomb stick/slip cap test in FP64.
+ *   RP_PRECISION_FP64_VERDICT near-boundary hold/slide classification in FP64. */
+typedef enum rp_precision {
+    RP_PRECISION_REFERENCE = 0,
+    RP_PRECISION_COMPENSATED = 1,
+    RP_PRECISION_FP64_CONE = 2,
+    RP_PRECISION_FP64_VERDICT = 4
+} rp_precision;
+
+/* Primitive types (reference: TPrimitive::Type, geometry.h:19). */
+enum { RP_PRIM_PLANE = 0, RP_PRIM_SPHERE = 1, RP_PRIM_CAPSULE = 2, RP_PRIM_BOX = 3 };
+
+/* Contact slot states written by rp_batch_read_contact_states. */
+enum {
+    RP_CONTACT_NONE = 0,      /* no contact generated for this (particle, primitive) */
+    RP_CONTACT_SEPARATED = 1, /* generated (within the margin) but not pushing */
+    RP_CONTACT_STICK = 2,     /* pushing; friction undid all tangential motion */
+    RP_CONTACT_SLIP = 3       /* pushing; friction capped by the Coulomb cone */
+};
+
+/* Isotropic circular section (reference: RodMaterial, rod.h:26-45). */
+typedef struct rp_material {
+    double youngs;  /* E [Pa] */
+    double poisson; /* nu */
+    double density; /* rho [kg/m^3] */
+    double radius;  /* r [m] */
+} rp_material;
+
+/* One rod as structure-of-arrays, double precision (reference: Rod,
+ * rod.h:49-121). Counts: P particles, S frames (segments plus ghost frames),
+ * St stretch constraints, B bend constraints. Arrays that may be NULL on
+ * input are marked; a NULL load array means zero. */
+typedef struct rp_rod_desc {
+    int32_t num_particles, num_frames, num_stretch, num_bend;
+    rp_material material;
+    /* particles */
+    double* x;              /* 3P */
+    double* v;              /* 3P */
+    double* inv_mass;       /* P, 0 = pinned */
+    double* mass;           /* P (may be NULL) */
+    double* ext_force;      /* 3P (may be NULL) */
+    double* kin_velocity;   /* 3P: velocity a pinned particle moves at (may be NULL) */
+    /* frames */
+    double* q;              /* 4S */
+    double* omega;          /* 3S, body frame */
+    double* inertia;        /* 3S, body-frame diagonal */
+    double* inv_inertia;    /* 3S, 0 = fixed (ghost) frame */
+    double* ext_torque;     /* 3S, world frame (may be NULL) */
+    /* stretch/shear constraints */
+    int32_t* s_p0;          /* St */
+    int32_t* s_p1;          /* St */
+    int32_t* s_seg;         /* St */
+    double* s_rest;         /* St */
+    double* s_compliance;   /* 3St */
+    /* bend/twist constraints */
+    int32_t* b_a;           /* B */
+    int32_t* b_b;           /* B */
+    double* b_rest;         /* B */
+    double* b_compliance;   /* 3B */
+    double* b_rest_darboux; /* 3B */
+} rp_rod_desc;
+
+/* Analytic primitive (reference: TPrimitive, geometry.h:17-65). */
+typedef struct rp_primitive {
+    int32_t type;
+    int32_t reserved;
+    double a[3];            /* plane point / sphere centre / capsule end A / box centre */
+    double b[3];            /* capsule end B */
+    double normal[3];       /* plane unit normal */
+    double half_extents[3]; /* box */
+    double rotation[4];     /* box orientation, wxyz */
+    double radius;          /* sphere / capsule */
+    double friction;
+} rp_primitive;
+
+/* Collision world (reference: CollisionWorld, collision.h:83-106). */
+typedef struct rp_world {
+    const rp_primitive* primitives;
+    int32_t num_primitives;
+    int32_t self_collision;
+    double self_friction;
+    int32_t self_skip;            /* default 2 */
+    int32_t hash_table_size;      /* default 4096 (use a small table, e.g. 256) */
+    double contact_margin_radii;  /* default 0.25 */
+} rp_world;
+
+/* Step parameters (reference: BatchParams, gpu_solver.h:52-60). */
+typedef struct rp_step_params {
+    float dt;
+    int32_t substeps;
+    int32_t iterations;
+    float gravity[3];
+    float linear_damping;
+    float angular_damping;
+    int32_t contact_interval;
+} rp_step_params;
+
+/* On-device drive of one rod's pinned particle (no host upload per step):
+ * the particle moves along `axis` with displacement A sin(2 pi f t + phase),
+ * i.e. its kinematic velocity is A 2 pi f cos(2 pi f t + phase) evaluated at
+ * the start of each substep. particle < 0 disables the drive for the rod. */
+typedef struct rp_drive {
+    int32_t particle;
+    int32_t reserved;
+    float axis[3];
+    float amplitude; /* [m] */
+    float frequency; /* [Hz] */
+    float phase;     /* [rad] */
+} rp_drive;
+
+typedef struct rp_rod rp_rod;     /* host-side rod descriptor owned by the library */
+typedef struct rp_batch rp_batch; /* device-resident batch */
+
+/* ------------------------------------------------------------------ device */
+/* reference: cudaAvailable(), deviceName(), diagnostic(), gpu_solver.h:44-48 */
+int32_t rp_cuda_available(void);
+rp_status rp_device_name(char* out, size_t capacity);
+rp_status rp_diagnostic(char* out, size_t capacity);
+/* reference: maxFusedSegments(), gpu_solver.h:150 (here with the 227 KB
+ * opt-in shared memory of sm_100, for a free rod without contacts). */
+int32_t rp_max_fused_segments(void);
+/* Message of the last failure on the calling thread ("" if none). */
+const char* rp_last_error(void);
+int32_t rp_abi_version(void);
+
+/* ------------------------------------------------------------------ rods */
+/* reference: makeStraightRod, rod.h:126-127 */
+rp_status rp_rod_create_straight(int32_t num_segments, double length, const rp_material* material,
+                                 const double origin[3], const double direction[3], rp_rod** out);
+/* reference: makeRodFromCenterline, rod.h:133-134 */
+rp_status rp_rod_create_centerline(const double* points, int32_t num_points,
+                                   const rp_material* material, const double frame_seed[3],
+                                   double twist_per_length, rp_rod** out);
+/* Deep copy of caller-owned arrays (any topology). */
+rp_status rp_rod_create_from_desc(const rp_rod_desc* desc, rp_rod** out);
+void rp_rod_destroy(rp_rod* rod);
+/* Mutable view of the rod's arrays (valid until the next call that changes
+ * its sizes: rp_rod_clamp_end). reference: the public fields of Rod. */
+rp_status rp_rod_view(rp_rod* rod, rp_rod_desc* out);
+/* reference: clampEndExact, rod.h:160; returns the ghost frame index. */
+rp_status rp_rod_clamp_end(rp_rod* rod, int32_t tip, int32_t* ghost_frame);
+/* reference: Rod::pinParticle, rod.h:109 */
+rp_status rp_rod_pin_particle(rp_rod* rod, int32_t particle);
+/* reference: setRestFromCurrent, rod.h:167 */
+rp_status rp_rod_set_rest_from_current(rp_rod* rod);
+
+/* ------------------------------------------------------------------ colouring */
+/* reference: colorStretchConstraints / colorBendConstraints, coloring.h:41-42.
+ * order: num_stretch (or num_bend) entries; color_start: capacity count + 1. */
+rp_status rp_rod_coloring(const rp_rod_desc* rod, int32_t bend, int32_t* order,
+                          int32_t* color_start, int32_t* num_colors);
+/* reference: colorConstraints, coloring.h:37. resources of constraint k are
+ * resources[resource_start[k] .. resource_start[k+1]). */
+rp_status rp_color_constraints(int32_t count, const int32_t* resource_start,
+                               const int32_t* resources, int32_t* order, int32_t* color_start,
+                               int32_t* num_colors);
+/* reference: selfCollisionIndexGap, collision.h:117 */
+rp_status rp_self_collision_index_gap(const rp_rod_desc* rod, const rp_world* world, int32_t* gap);
+
+/* ------------------------------------------------------------------ batch */
+/* reference: Batch::create(prototype, numRods, strategy, world),
+ * gpu_solver.h:81-82, gpu_batch.cpp:150-316. Every rod is a copy of the
+ * prototype and collides with `world` (NULL = no contacts). */
+rp_status rp_batch_create(const rp_rod_desc* prototype, int32_t num_rods, rp_strategy strategy,
+                          const rp_world* world, rp_batch** out);
+/* Heterogeneous batch (no reference counterpart: the reference batch shares
+ * one prototype and one world). rods[i] is rod i's descriptor; rods that pass
+ * the same pointer share their topology and rest data on the device.
+ * world_of_rod[i] indexes `worlds` (NULL: every rod uses worlds[0], or no
+ * world when num_worlds is 0). */
+rp_status rp_batch_create_mixed(const rp_rod_desc* const* rods, int32_t num_rods,
+                                const rp_world* worlds, int32_t num_worlds,
+                                const int32_t* world_of_rod, rp_strategy strategy,
+                                rp_batch** out);
+/* reference: Batch::destroy / ~Batch, gpu_solver.h:83, gpu_batch.cpp:132-138 */
+void rp_batch_destroy(rp_batch* batch);
+/* reference: Batch::step, gpu_solver.h:85, gpu_batch.cpp:457-473 */
+rp_status rp_batch_step(rp_batch* batch, const rp_step_params* params);
+/* `steps` steps; when graphs are enabled (rp_batch_set_graph) the sequence is
+ * replayed from a captured CUDA graph. */
+rp_status rp_batch_step_many(rp_batch* batch, const rp_step_params* params, int32_t steps);
+/* reference: Batch::synchronize, gpu_solver.h:86 */
+rp_status rp_batch_synchronize(rp_batch* batch);
+/* Run the batch on a caller-owned cudaStream_t (NULL = the library's own). */
+rp_status rp_batch_set_stream(rp_batch* batch, void* cuda_stream);
+rp_status rp_batch_set_precision(rp_batch* batch, int32_t flags);
+/* Capture rp_batch_step_many sequences into CUDA graphs (1) or launch
+ * directly (0, default). */
+rp_status rp_batch_set_graph(rp_batch* batch, int32_t enabled);
+
+/* reference: Batch::download(rodIndex, Rod&), gpu_solver.h:90. Writes x, v,
+ * q and omega of rod `rod` into `out`'s arrays (same topology). */
+rp_status rp_batch_download(rp_batch* batch, int32_t rod, rp_rod_desc* out);
+/* reference: Batch::downloadPositions, gpu_solver.h:94. Rod-major xyz floats:
+ * out[(particle_offset(rod) + i) * 3 + c]; for a homogeneous batch that is
+ * out[(rod * particles + i) * 3 + c], as in the reference. */
+rp_status rp_batch_download_positions(rp_batch* batch, float* out, int64_t capacity_floats);
+/* Rod-major quaternion frames, wxyz floats, same ordering as positions. */
+rp_status rp_batch_download_frames(rp_batch* batch, float* out, int64_t capacity_floats);
+/* reference: Batch::upload(const Rod&), gpu_solver.h:97 (every rod) */
+rp_status rp_batch_upload(rp_batch* batch, const rp_rod_desc* rod);
+/* reference: Batch::setLoads, gpu_solver.h:102 */
+rp_status rp_batch_set_loads(rp_batch* batch, int32_t rod, const rp_rod_desc* source);
+/* reference: Batch::uploadRod, gpu_solver.h:105 */
+rp_status rp_batch_upload_rod(rp_batch* batch, int32_t rod, const rp_rod_desc* source);
+/* reference: Batch::setKinematicVelocities, gpu_solver.h:109 (rod-major xyz) */
+rp_status rp_batch_set_kinematic_velocities(rp_batch* batch, const float* rod_major_xyz,
+                                            int64_t count_vec3);
+/* reference: Batch::setMaterialScales, gpu_solver.h:114-115. Either pointer
+ * may be NULL to leave that scale at its current value; n must be numRods. */
+rp_status rp_batch_set_material_scales(rp_batch* batch, const float* youngs_scale,
+                                       const float* friction_scale, int32_t n);
+/* On-device drives, one per rod (n = numRods); NULL clears them. */
+rp_status rp_batch_set_drives(rp_batch* batch, const rp_drive* drives, int32_t n);
+/* Simulated time the drives are evaluated at (advanced by every step). */
+rp_status rp_batch_set_time(rp_batch* batch, double time);
+
+/* Raw asynchronous copies between the device state and caller memory, on
+ * the batch's stream (no reference counterpart: the reference copies
+ * synchronously and reorders on the host). Use pinned host memory for full
+ * speed and rp_batch_synchronize() before reading what was copied. Rows are
+ * 16-byte float4 in particle_offset / frame_offset order:
+ *   RP_STATE_POSITIONS  read   xyz_ per particle (compensated mode: the
+ *                              rounded sum, without its compensation term)
+ *   RP_STATE_FRAMES     read   wxyz per frame
+ *   RP_STATE_CONTACTS   read   one RP_CONTACT_* byte per slot
+ *   RP_STATE_KINEMATIC  write  xyz_ kinematic velocity per particle
+ * `bytes` must equal the whole array's size. */
+enum { RP_STATE_POSITIONS = 0, RP_STATE_FRAMES = 1, RP_STATE_CONTACTS = 2, RP_STATE_KINEMATIC = 3 };
+rp_status rp_batch_read_state_async(rp_batch* batch, int32_t what, void* dst, int64_t bytes);
+rp_status rp_batch_write_state_async(rp_batch* batch, int32_t what, const void* src, int64_t bytes);
+
+/* Per (rod, particle, primitive) contact state at the end of the last step,
+ * RP_CONTACT_*; layout rod-major: (particle_offset(rod) + i) * prims + k where
+ * prims is the rod's primitive count. Returns the total slot count in *count. */
+rp_status rp_batch_read_contact_states(rp_batch* batch, uint8_t* out, int64_t capacity,
+                                       int64_t* count);
+/* Self-contact pairs (segment j, segment k) of the last contact regeneration
+ * of `rod`, in projection order. */
+rp_status rp_batch_read_self_contacts(rp_batch* batch, int32_t rod, int32_t* pairs_jk,
+                                      int32_t capacity, int32_t* count);
+
+/* Hold/slide observation (reference: HangOutcome, apps/cable_hanging.h:68-77):
+ * every `interval` steps each rod's `particle` z is compared with its z at
+ * arming time; held = max rise <= tolerance. particle < 0 disarms. */
+rp_status rp_batch_arm_hold_observer(rp_batch* batch, const int32_t* particle_of_rod,
+                                     int32_t n, int32_t interval, double tolerance);
+/* max_rise (may be NULL) and held (may be NULL), one per rod; near_boundary
+ * (may be NULL) flags rods whose max rise lies within float resolution of the
+ * tolerance, classified in FP64 when RP_PRECISION_FP64_VERDICT is set. */
+rp_status rp_batch_read_hold_verdicts(rp_batch* batch, double* max_rise, uint8_t* held,
+                                      uint8_t* near_boundary, int32_t n);
+
+/* accessors (reference: gpu_solver.h:117-130) */
+int32_t rp_batch_num_rods(const rp_batch* batch);
+int32_t rp_batch_num_segments(const rp_batch* batch, int32_t rod);
+int32_t rp_batch_num_particles(const rp_batch* batch, int32_t rod);
+int64_t rp_batch_particle_offset(const rp_batch* batch, int32_t rod);
+int32_t rp_batch_num_frames(const rp_batch* batch, int32_t rod);
+int64_t rp_batch_frame_offset(const rp_batch* batch, int32_t rod);
+int32_t rp_batch_strategy(const rp_batch* batch);
+int32_t rp_batch_stretch_colors(const rp_batch* batch);
+int32_t rp_batch_bend_colors(const rp_batch* batch);
+size_t rp_batch_shared_bytes_per_block(const rp_batch* batch);
+int32_t rp_batch_launches_per_step(const rp_batch* batch, const rp_step_params* params);
+int64_t rp_batch_self_contact_overflow(rp_batch* batch);
+/* Kernel launches issued by this batch since creation (for accounting). */
+int64_t rp_batch_kernel_launches(const rp_batch* batch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ROPEPHYSICS_B200_H */

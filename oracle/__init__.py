@@ -76,7 +76,7 @@ def _contact_struct(real):
         _fields_ = [("idx", C.c_int32 * 4), ("weight", real * 4), ("normal", real * 3),
                     ("offset", real), ("friction", real), ("lambdaN", real),
                     ("appliedTangential", real), ("count", C.c_int32),
-                    ("frictionState", C.c_int32)]
+                    ("frictionState", C.c_int32), ("prim", C.c_int32), ("pad", C.c_int32)]
     return OrcContact
 
 
@@ -275,7 +275,8 @@ class Context:
             k = self.buf[i]
             out.append(dict(idx=tuple(k.idx[: k.count]), weight=tuple(k.weight[: k.count]),
                             normal=tuple(k.normal), offset=k.offset, friction=k.friction,
-                            lambdaN=k.lambdaN, count=k.count, friction_state=k.frictionState))
+                            lambdaN=k.lambdaN, count=k.count, friction_state=k.frictionState,
+                            prim=k.prim))
         return out
 
 
@@ -510,6 +511,17 @@ class Reference:
         self.lib.ref_step(h, world_handle, p.dt, p.substeps, p.iterations,
                           Oracle._d3(p.gravity), p.linear_damping, p.angular_damping,
                           p.contact_interval, int(colored), steps)
+
+    def contacts(self, h, cap=8192):
+        """The contact list the rod's last substep used (its SolverContext)."""
+        idx = np.zeros((cap, 4), np.int32)
+        w = np.zeros((cap, 4))
+        n = np.zeros((cap, 3))
+        off = np.zeros(cap)
+        D = C.POINTER(C.c_double)
+        cnt = self.lib.ref_contacts(h, idx.ctypes.data_as(C.POINTER(C.c_int)), w.ctypes.data_as(D),
+                                    n.ctypes.data_as(D), off.ctypes.data_as(D), cap)
+        return idx[:cnt], w[:cnt], n[:cnt], off[:cnt]
 
     def generate_contacts(self, h, world_handle, cap=8192):
         idx = np.zeros((cap, 4), np.int32)

@@ -519,6 +519,8 @@ void pushContact(orc_context* ctx, const orc_rod* rod, const int* idx, const R* 
     c.lambdaN = R(0);
     c.appliedTangential = R(0);
     c.frictionState = 0;
+    c.prim = -1;
+    c.pad = 0;
     R dotSum = R(0);
     for (int k = 0; k < 4; ++k) {
         c.idx[k] = -1;
@@ -548,6 +550,8 @@ void generateContacts(const orc_rod* rod, const orc_world* world, orc_context* c
             const int idx[1] = {i};
             const R w[1] = {R(1)};
             pushContact(ctx, rod, idx, w, 1, n, gap, prims[k].friction);
+            if (ctx->count > 0 && ctx->contacts[ctx->count - 1].idx[0] == int(i))
+                ctx->contacts[ctx->count - 1].prim = k;
         }
     }
     if (!world->selfCollision) return;

@@ -93,6 +93,8 @@ typedef struct orc_contact {
      * 0 none (separated or frictionless), 1 stick, 2 slip. Not part of the
      * reference struct; derived from the cap test in projectContacts. */
     int32_t frictionState;
+    int32_t prim; /* primitive index (world contacts), -1 for self contacts */
+    int32_t pad;
 } orc_contact;
 
 /* SolverParams (src/core/solver.h:15-37). */

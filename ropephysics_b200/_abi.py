@@ -1,0 +1,146 @@
+"""ctypes declarations of the C ABI in ``include/ropephysics_b200.h``.
+
+``load()`` opens the in-tree ``librp_b200.so`` and declares every exported
+function. There is no fallback: if the library is missing the import fails
+with the build command to run.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "librp_b200.so")
+
+i32, i64, f32, f64, u8 = C.c_int32, C.c_int64, C.c_float, C.c_double, C.c_uint8
+P = C.POINTER
+
+
+class Material(C.Structure):
+    _fields_ = [("youngs", f64), ("poisson", f64), ("density", f64), ("radius", f64)]
+
+
+class RodDesc(C.Structure):
+    _fields_ = [
+        ("num_particles", i32), ("num_frames", i32), ("num_stretch", i32), ("num_bend", i32),
+        ("material", Material),
+        ("x", P(f64)), ("v", P(f64)), ("inv_mass", P(f64)), ("mass", P(f64)),
+        ("ext_force", P(f64)), ("kin_velocity", P(f64)),
+        ("q", P(f64)), ("omega", P(f64)), ("inertia", P(f64)), ("inv_inertia", P(f64)),
+        ("ext_torque", P(f64)),
+        ("s_p0", P(i32)), ("s_p1", P(i32)), ("s_seg", P(i32)), ("s_rest", P(f64)),
+        ("s_compliance", P(f64)),
+        ("b_a", P(i32)), ("b_b", P(i32)), ("b_rest", P(f64)), ("b_compliance", P(f64)),
+        ("b_rest_darboux", P(f64)),
+    ]
+
+
+class Primitive(C.Structure):
+    _fields_ = [("type", i32), ("reserved", i32), ("a", f64 * 3), ("b", f64 * 3),
+                ("normal", f64 * 3), ("half_extents", f64 * 3), ("rotation", f64 * 4),
+                ("radius", f64), ("friction", f64)]
+
+
+class World(C.Structure):
+    _fields_ = [("primitives", P(Primitive)), ("num_primitives", i32), ("self_collision", i32),
+                ("self_friction", f64), ("self_skip", i32), ("hash_table_size", i32),
+                ("contact_margin_radii", f64)]
+
+
+class StepParams(C.Structure):
+    _fields_ = [("dt", f32), ("substeps", i32), ("iterations", i32), ("gravity", f32 * 3),
+                ("linear_damping", f32), ("angular_damping", f32), ("contact_interval", i32)]
+
+
+class Drive(C.Structure):
+    _fields_ = [("particle", i32), ("reserved", i32), ("axis", f32 * 3), ("amplitude", f32),
+                ("frequency", f32), ("phase", f32)]
+
+
+vp = C.c_void_p
+pp = P(vp)
+
+# name: (restype, argtypes) -- one entry per declaration in the header
+SIGNATURES = {
+    "rp_abi_version": (i32, []),
+    "rp_cuda_available": (i32, []),
+    "rp_device_name": (i32, [C.c_char_p, C.c_size_t]),
+    "rp_diagnostic": (i32, [C.c_char_p, C.c_size_t]),
+    "rp_max_fused_segments": (i32, []),
+    "rp_last_error": (C.c_char_p, []),
+    "rp_rod_create_straight": (i32, [i32, f64, P(Material), P(f64), P(f64), pp]),
+    "rp_rod_create_centerline": (i32, [P(f64), i32, P(Material), P(f64), f64, pp]),
+    "rp_rod_create_from_desc": (i32, [P(RodDesc), pp]),
+    "rp_rod_destroy": (None, [vp]),
+    "rp_rod_view": (i32, [vp, P(RodDesc)]),
+    "rp_rod_clamp_end": (i32, [vp, i32, P(i32)]),
+    "rp_rod_pin_particle": (i32, [vp, i32]),
+    "rp_rod_set_rest_from_current": (i32, [vp]),
+    "rp_rod_coloring": (i32, [P(RodDesc), i32, P(i32), P(i32), P(i32)]),
+    "rp_color_constraints": (i32, [i32, P(i32), P(i32), P(i32), P(i32), P(i32)]),
+    "rp_self_collision_index_gap": (i32, [P(RodDesc), P(World), P(i32)]),
+    "rp_batch_create": (i32, [P(RodDesc), i32, i32, P(World), pp]),
+    "rp_batch_create_mixed": (i32, [P(P(RodDesc)), i32, P(World), i32, P(i32), i32, pp]),
+    "rp_batch_destroy": (None, [vp]),
+    "rp_batch_step": (i32, [vp, P(StepParams)]),
+    "rp_batch_step_many": (i32, [vp, P(StepParams), i32]),
+    "rp_batch_synchronize": (i32, [vp]),
+    "rp_batch_set_stream": (i32, [vp, vp]),
+    "rp_batch_set_precision": (i32, [vp, i32]),
+    "rp_batch_set_graph": (i32, [vp, i32]),
+    "rp_batch_download": (i32, [vp, i32, P(RodDesc)]),
+    "rp_batch_download_positions": (i32, [vp, P(f32), i64]),
+    "rp_batch_download_frames": (i32, [vp, P(f32), i64]),
+    "rp_batch_upload": (i32, [vp, P(RodDesc)]),
+    "rp_batch_set_loads": (i32, [vp, i32, P(RodDesc)]),
+    "rp_batch_upload_rod": (i32, [vp, i32, P(RodDesc)]),
+    "rp_batch_set_kinematic_velocities": (i32, [vp, P(f32), i64]),
+    "rp_batch_set_material_scales": (i32, [vp, P(f32), P(f32), i32]),
+    "rp_batch_set_drives": (i32, [vp, P(Drive), i32]),
+    "rp_batch_set_time": (i32, [vp, f64]),
+    "rp_batch_read_state_async": (i32, [vp, i32, vp, i64]),
+    "rp_batch_write_state_async": (i32, [vp, i32, vp, i64]),
+    "rp_batch_read_contact_states": (i32, [vp, P(u8), i64, P(i64)]),
+    "rp_batch_read_self_contacts": (i32, [vp, i32, P(i32), i32, P(i32)]),
+    "rp_batch_arm_hold_observer": (i32, [vp, P(i32), i32, i32, f64]),
+    "rp_batch_read_hold_verdicts": (i32, [vp, P(f64), P(u8), P(u8), i32]),
+    "rp_batch_num_rods": (i32, [vp]),
+    "rp_batch_num_segments": (i32, [vp, i32]),
+    "rp_batch_num_particles": (i32, [vp, i32]),
+    "rp_batch_particle_offset": (i64, [vp, i32]),
+    "rp_batch_num_frames": (i32, [vp, i32]),
+    "rp_batch_frame_offset": (i64, [vp, i32]),
+    "rp_batch_strategy": (i32, [vp]),
+    "rp_batch_stretch_colors": (i32, [vp]),
+    "rp_batch_bend_colors": (i32, [vp]),
+    "rp_batch_shared_bytes_per_block": (C.c_size_t, [vp]),
+    "rp_batch_launches_per_step": (i32, [vp, P(StepParams)]),
+    "rp_batch_self_contact_overflow": (i64, [vp]),
+    "rp_batch_kernel_launches": (i64, [vp]),
+}
+
+_lib = None
+
+
+def load():
+    """Open the native library once and declare its functions."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: run `python -m ropephysics_b200.build`")
+    lib = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def header_symbols(header: str) -> list:
+    """Function names declared in the C header (for the export check)."""
+    import re
+    text = open(header).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(rp_[a-z0-9_]+)\s*\(", text)))

@@ -1,0 +1,1266 @@
+// rp_batch.cpp -- the device-resident batch behind the C ABI.
+//
+// Replaces the reference's host orchestration (src/gpu/gpu_batch.cpp:1-487)
+// and its device shims (src/gpu/gpu_solver.cu:742-799). Differences by design:
+//   * rods may differ in topology and world (rp_batch_create_mixed); rods made
+//     from one descriptor share a template on the device;
+//   * every CUDA call and launch is checked and reported through rp_status;
+//   * the batch runs on its own stream (or a caller's), uploads are batched
+//     into one copy per array instead of per element;
+//   * FUSED opts into the 227 KB of shared memory per block of sm_100.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "ropephysics_b200.h"
+#include "rp_host.h"
+#include "rp_internal.h"
+#include "rp_launch.h"
+#include "rp_layout.h"
+
+using rp::DArgs;
+using rp::DPrim;
+using rp::DRod;
+using rp::DTemplate;
+
+namespace {
+thread_local std::string g_lastError;
+}
+
+namespace rpx {
+rp_status fail(rp_status s, const std::string& msg) {
+    g_lastError = msg;
+    return s;
+}
+}  // namespace rpx
+
+using rpx::fail;
+
+#define RP_CUDA(call)                                                                     \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(RP_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+namespace {
+
+// Autotuned launch choices for the batched form (see rp_tune.cpp).
+struct Tune {
+    int ctaThreads = 256;
+    int pairsPerThread = 1;  // team threads ~ ceil(nSt / 2 / pairsPerThread), rounded to 32
+};
+
+float4 f4(double a, double b, double c, double d = 0.0) {
+    return make_float4(float(a), float(b), float(c), float(d));
+}
+
+}  // namespace
+
+struct rp_batch {
+    int device = 0;
+    rp_strategy strategy = RP_STRATEGY_FUSED;
+    int numRods = 0;
+    int precision = 0;
+    cudaStream_t stream = nullptr;
+    bool ownStream = false;
+    int plainThreads = 128;
+    size_t smemBytes = 0;
+    int maxPrims = 0;
+    bool anySelf = false;
+    int sColorsMax = 0, bColorsMax = 0;
+    long long launches = 0;
+
+    std::vector<DTemplate> tmpls;
+    std::vector<DRod> rods;
+    std::vector<int> tmplNP;        // per rod particles (host copy)
+    std::vector<int> tmplNS;        // per rod frames
+    std::vector<std::vector<char>> fixedFrame;  // per template: frame is fixed (zero inertia)
+    int64_t totalP = 0, totalS = 0, totalSt = 0, totalB = 0, totalSlots = 0;
+    int64_t totalPool = 0, totalHash = 0;
+
+    std::vector<void*> owned;
+    DArgs a{};
+    int32_t* dWork = nullptr;
+
+    // batched plan
+    std::vector<int32_t> groups;  // 4 ints per group
+    int32_t* dGroups = nullptr;
+    int32_t* dQueue = nullptr;
+    int numGroups = 0;
+    int batchedBlocks = 0;
+    int batchedThreads = 256;
+    size_t batchedSmem = 0;
+    Tune tune;
+
+    // graphs
+    bool useGraph = false;
+    cudaGraphExec_t graphExec = nullptr;
+    int graphSteps = 0;
+    rp_step_params graphParams{};
+    int graphPrecision = -1;
+
+    // hold observer
+    int holdInterval = 0;
+    double holdTolerance = 0.05;
+    bool holdArmed = false;
+
+    ~rp_batch() {
+        if (graphExec) cudaGraphExecDestroy(graphExec);
+        for (void* p : owned) cudaFree(p);
+        if (ownStream && stream) cudaStreamDestroy(stream);
+    }
+
+    template <typename T>
+    rp_status alloc(T*& out, size_t count, bool zero = true) {
+        out = nullptr;
+        if (count == 0) count = 1;
+        void* p = nullptr;
+        const cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(RP_ERR_OUT_OF_MEMORY, "cudaMalloc of " + std::to_string(count * sizeof(T)) +
+                                                  " bytes failed: " + cudaGetErrorString(e));
+        }
+        owned.push_back(p);
+        if (zero) {
+            const cudaError_t z = cudaMemsetAsync(p, 0, count * sizeof(T), stream);
+            if (z != cudaSuccess) return fail(RP_ERR_CUDA, cudaGetErrorString(z));
+        }
+        out = static_cast<T*>(p);
+        return RP_OK;
+    }
+
+    template <typename T>
+    rp_status upload(T* dst, const std::vector<T>& src) {
+        if (src.empty()) return RP_OK;
+        RP_CUDA(cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
+        return RP_OK;
+    }
+};
+
+namespace {
+
+bool deviceUsable(std::string* why) {
+    int n = 0;
+    const cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        if (why) {
+            int rt = 0, dr = 0;
+            cudaRuntimeGetVersion(&rt);
+            cudaDriverGetVersion(&dr);
+            *why = std::string("no usable CUDA device: error ") + std::to_string(int(e)) + " (" +
+                   cudaGetErrorString(e) + "); runtime CUDA " + std::to_string(rt / 1000) + "." +
+                   std::to_string((rt % 1000) / 10) + ", driver supports CUDA " +
+                   std::to_string(dr / 1000) + "." + std::to_string((dr % 1000) / 10);
+        }
+        cudaGetLastError();
+        return false;
+    }
+    return true;
+}
+
+size_t optinSmem(int device) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess) {
+        cudaGetLastError();
+        return 48 * 1024;
+    }
+    return size_t(v);
+}
+
+DPrim toDPrim(const rp_primitive& p) {
+    DPrim d{};
+    d.ax = float(p.a[0]);
+    d.ay = float(p.a[1]);
+    d.az = float(p.a[2]);
+    d.radius = float(p.radius);
+    d.bx = float(p.b[0]);
+    d.by = float(p.b[1]);
+    d.bz = float(p.b[2]);
+    d.friction = float(p.friction);
+    d.nx = float(p.normal[0]);
+    d.ny = float(p.normal[1]);
+    d.nz = float(p.normal[2]);
+    d.typef = float(p.type);
+    d.hx = float(p.half_extents[0]);
+    d.hy = float(p.half_extents[1]);
+    d.hz = float(p.half_extents[2]);
+    d.qw = float(p.rotation[0]);
+    d.qx = float(p.rotation[1]);
+    d.qy = float(p.rotation[2]);
+    d.qz = float(p.rotation[3]);
+    return d;
+}
+
+std::string validateWorld(const rp_world& w) {
+    if (w.num_primitives < 0 || (w.num_primitives > 0 && !w.primitives))
+        return "world has primitives but a NULL array";
+    if (w.num_primitives > 64) return "at most 64 primitives per world";
+    for (int k = 0; k < w.num_primitives; ++k) {
+        const rp_primitive& p = w.primitives[k];
+        if (p.type < 0 || p.type > 3) return "primitive type must be 0..3";
+        if ((p.type == 1 || p.type == 2) && !(p.radius >= 0)) return "negative primitive radius";
+    }
+    if (w.self_collision && (w.hash_table_size < 1 || w.hash_table_size > (1 << 20)))
+        return "self-collision needs 1 <= hash_table_size <= 2^20";
+    return "";
+}
+
+// Chain topology: stretch k = (k, k+1, frame k); bends 0..nSt-2 = (k, k+1);
+// any further bends involve a ghost frame (index >= nSt).
+int isChain(const rp_rod_desc* d) {
+    if (d->num_particles != d->num_stretch + 1) return 0;
+    for (int k = 0; k < d->num_stretch; ++k)
+        if (d->s_p0[k] != k || d->s_p1[k] != k + 1 || d->s_seg[k] != k) return 0;
+    if (d->num_bend < d->num_stretch - 1) return 0;
+    for (int k = 0; k < d->num_stretch - 1; ++k)
+        if (d->b_a[k] != k || d->b_b[k] != k + 1) return 0;
+    for (int k = d->num_stretch - 1; k < d->num_bend; ++k)
+        if (d->b_a[k] < d->num_stretch && d->b_b[k] < d->num_stretch) return 0;
+    return 1;
+}
+
+// Per-rod state upload helpers: double descriptor -> float4 rows.
+void packParticles(const rp_rod_desc* d, float4* x, float4* v, float4* f, float4* k) {
+    for (int i = 0; i < d->num_particles; ++i) {
+        if (x) x[i] = f4(d->x[3 * i], d->x[3 * i + 1], d->x[3 * i + 2]);
+        if (v) v[i] = d->v ? f4(d->v[3 * i], d->v[3 * i + 1], d->v[3 * i + 2]) : f4(0, 0, 0);
+        if (f)
+            f[i] = d->ext_force ? f4(d->ext_force[3 * i], d->ext_force[3 * i + 1], d->ext_force[3 * i + 2])
+                                : f4(0, 0, 0);
+        if (k)
+            k[i] = d->kin_velocity
+                       ? f4(d->kin_velocity[3 * i], d->kin_velocity[3 * i + 1], d->kin_velocity[3 * i + 2])
+                       : f4(0, 0, 0);
+    }
+}
+void packFrames(const rp_rod_desc* d, float4* q, float4* w, float4* t) {
+    for (int j = 0; j < d->num_frames; ++j) {
+        if (q) q[j] = f4(d->q[4 * j], d->q[4 * j + 1], d->q[4 * j + 2], d->q[4 * j + 3]);
+        if (w) w[j] = d->omega ? f4(d->omega[3 * j], d->omega[3 * j + 1], d->omega[3 * j + 2]) : f4(0, 0, 0);
+        if (t)
+            t[j] = d->ext_torque ? f4(d->ext_torque[3 * j], d->ext_torque[3 * j + 1], d->ext_torque[3 * j + 2])
+                                 : f4(0, 0, 0);
+    }
+}
+
+bool sameTopology(const rp_batch* b, int r, const rp_rod_desc* d) {
+    return d && d->num_particles == b->tmplNP[r] && d->num_frames == b->tmplNS[r];
+}
+
+rp_status buildBatchedPlan(rp_batch* b);
+
+}  // namespace
+
+// ---------------------------------------------------------------- create
+
+static rp_status createImpl(const rp_rod_desc* const* rods, int numRods, const rp_world* worlds,
+                            int numWorlds, const int32_t* worldOfRod, rp_strategy strategy,
+                            rp_batch** out) {
+    if (!out) return fail(RP_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (numRods < 1) return fail(RP_ERR_INVALID, "num_rods must be >= 1");
+    if (strategy < RP_STRATEGY_MULTI_KERNEL || strategy > RP_STRATEGY_BATCHED)
+        return fail(RP_ERR_INVALID, "unknown strategy");
+    if (numWorlds < 0 || (numWorlds > 0 && !worlds)) return fail(RP_ERR_INVALID, "bad worlds");
+    for (int w = 0; w < numWorlds; ++w) {
+        const std::string why = validateWorld(worlds[w]);
+        if (!why.empty()) return fail(RP_ERR_INVALID, "world " + std::to_string(w) + ": " + why);
+    }
+    for (int r = 0; r < numRods; ++r) {
+        if (worldOfRod && (worldOfRod[r] < 0 || worldOfRod[r] >= std::max(numWorlds, 1) ||
+                           (numWorlds == 0 && worldOfRod[r] != 0)))
+            return fail(RP_ERR_INVALID, "world_of_rod[" + std::to_string(r) + "] out of range");
+    }
+    std::string why;
+    if (!deviceUsable(&why)) return fail(RP_ERR_NO_DEVICE, why);
+
+    auto* b = new rp_batch();
+    auto guard = [&](rp_status s) {
+        delete b;
+        return s;
+    };
+    b->strategy = strategy;
+    b->numRods = numRods;
+    if (cudaGetDevice(&b->device) != cudaSuccess) return guard(fail(RP_ERR_CUDA, "cudaGetDevice failed"));
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return guard(fail(RP_ERR_CUDA, "cudaStreamCreate failed"));
+    b->ownStream = true;
+
+    // ---- templates (deduplicated by descriptor pointer) ----
+    std::map<const rp_rod_desc*, int> tmplOf;
+    std::vector<const rp_rod_desc*> tdesc;
+    std::vector<int> rodTmpl(numRods);
+    for (int r = 0; r < numRods; ++r) {
+        const rp_rod_desc* d = rods[r];
+        auto it = tmplOf.find(d);
+        if (it == tmplOf.end()) {
+            const std::string w = rpx::validateDesc(d);
+            if (!w.empty()) return guard(fail(RP_ERR_INVALID, "rod " + std::to_string(r) + ": " + w));
+            const int t = int(tdesc.size());
+            tmplOf[d] = t;
+            tdesc.push_back(d);
+            rodTmpl[r] = t;
+        } else {
+            rodTmpl[r] = it->second;
+        }
+    }
+    std::vector<float> tInvMass;
+    std::vector<float4> tInvInertia, tInertia, tSComp, tBComp, tBRestD;
+    std::vector<int32_t> tSP0, tSP1, tSSeg, tBA, tBB, tOrder, tColorStart;
+    for (const rp_rod_desc* d : tdesc) {
+        DTemplate T{};
+        T.nP = d->num_particles;
+        T.nS = d->num_frames;
+        T.nSt = d->num_stretch;
+        T.nB = d->num_bend;
+        T.pOff = int(tInvMass.size());
+        T.sOff = int(tInvInertia.size());
+        T.stOff = int(tSP0.size());
+        T.bOff = int(tBA.size());
+        for (int i = 0; i < T.nP; ++i) tInvMass.push_back(float(d->inv_mass[i]));
+        std::vector<char> fixed(T.nS, 0);
+        for (int j = 0; j < T.nS; ++j) {
+            const double* iI = d->inv_inertia + 3 * j;
+            tInvInertia.push_back(f4(iI[0], iI[1], iI[2]));
+            tInertia.push_back(f4(d->inertia[3 * j], d->inertia[3 * j + 1], d->inertia[3 * j + 2]));
+            fixed[j] = (iI[0] * iI[0] + iI[1] * iI[1] + iI[2] * iI[2]) == 0.0;
+        }
+        b->fixedFrame.push_back(fixed);
+        for (int k = 0; k < T.nSt; ++k) {
+            tSP0.push_back(d->s_p0[k]);
+            tSP1.push_back(d->s_p1[k]);
+            tSSeg.push_back(d->s_seg[k]);
+            tSComp.push_back(f4(d->s_compliance[3 * k], d->s_compliance[3 * k + 1],
+                                d->s_compliance[3 * k + 2], d->s_rest[k]));
+        }
+        for (int k = 0; k < T.nB; ++k) {
+            tBA.push_back(d->b_a[k]);
+            tBB.push_back(d->b_b[k]);
+            tBComp.push_back(f4(d->b_compliance[3 * k], d->b_compliance[3 * k + 1],
+                                d->b_compliance[3 * k + 2], d->b_rest[k]));
+            tBRestD.push_back(f4(d->b_rest_darboux[3 * k], d->b_rest_darboux[3 * k + 1],
+                                 d->b_rest_darboux[3 * k + 2]));
+        }
+        std::vector<int> order, cs;
+        T.sColors = rpx::colorRod(d, false, order, cs);
+        T.sOrderOff = int(tOrder.size());
+        tOrder.insert(tOrder.end(), order.begin(), order.end());
+        T.sColorOff = int(tColorStart.size());
+        tColorStart.insert(tColorStart.end(), cs.begin(), cs.end());
+        T.bColors = rpx::colorRod(d, true, order, cs);
+        T.bOrderOff = int(tOrder.size());
+        tOrder.insert(tOrder.end(), order.begin(), order.end());
+        T.bColorOff = int(tColorStart.size());
+        tColorStart.insert(tColorStart.end(), cs.begin(), cs.end());
+        T.chain = isChain(d);
+        b->sColorsMax = std::max(b->sColorsMax, T.sColors);
+        b->bColorsMax = std::max(b->bColorsMax, T.bColors);
+        b->tmpls.push_back(T);
+    }
+
+    // ---- worlds ----
+    std::vector<DPrim> prims;
+    std::vector<int> worldPrimOff(std::max(numWorlds, 1), 0);
+    for (int w = 0; w < numWorlds; ++w) {
+        worldPrimOff[w] = int(prims.size());
+        for (int k = 0; k < worlds[w].num_primitives; ++k) prims.push_back(toDPrim(worlds[w].primitives[k]));
+    }
+
+    // ---- rods ----
+    std::map<std::pair<int, int>, int> gapCache;
+    b->rods.resize(numRods);
+    b->tmplNP.resize(numRods);
+    b->tmplNS.resize(numRods);
+    size_t maxLayout = 0;
+    for (int r = 0; r < numRods; ++r) {
+        const int t = rodTmpl[r];
+        const DTemplate& T = b->tmpls[t];
+        const rp_rod_desc* d = tdesc[t];
+        const int wi = numWorlds > 0 ? (worldOfRod ? worldOfRod[r] : 0) : -1;
+        DRod R{};
+        R.tmpl = t;
+        R.pOff = int(b->totalP);
+        R.sOff = int(b->totalS);
+        R.stOff = int(b->totalSt);
+        R.bOff = int(b->totalB);
+        R.radius = float(d->material.radius);
+        if (wi >= 0) {
+            const rp_world& W = worlds[wi];
+            R.primOff = worldPrimOff[wi];
+            R.numPrims = W.num_primitives;
+            R.contactMargin = float(W.contact_margin_radii * d->material.radius);
+            if (W.self_collision) {
+                R.selfCollision = 1;
+                auto key = std::make_pair(t, W.self_skip);
+                auto g = gapCache.find(key);
+                if (g == gapCache.end()) g = gapCache.emplace(key, rpx::selfGap(d, W.self_skip)).first;
+                R.selfGap = g->second;
+                R.selfFriction = float(W.self_friction);
+                R.hashTableSize = W.hash_table_size;
+                R.selfCapacity = std::max(16, T.nSt / 2);
+            }
+        }
+        R.slotOff = b->totalSlots;
+        R.poolOff = int(b->totalPool);
+        R.hashOff = int(b->totalHash);
+        b->totalP += T.nP;
+        b->totalS += T.nS;
+        b->totalSt += T.nSt;
+        b->totalB += T.nB;
+        b->totalSlots += int64_t(T.nP) * R.numPrims;
+        b->totalPool += R.selfCapacity;
+        b->totalHash += R.selfCollision ? R.hashTableSize + 1 : 0;
+        b->maxPrims = std::max(b->maxPrims, R.numPrims);
+        b->anySelf = b->anySelf || R.selfCollision;
+        const rp::RodLayout L = rp::rodLayout(T.nP, T.nS, T.nSt, T.nB, R.numPrims, R.selfCollision,
+                                              R.hashTableSize, R.selfCapacity);
+        maxLayout = std::max(maxLayout, size_t(L.bytes));
+        b->rods[r] = R;
+        b->tmplNP[r] = T.nP;
+        b->tmplNS[r] = T.nS;
+    }
+    if (b->totalP > (int64_t(1) << 31) - 1 || b->totalS > (int64_t(1) << 31) - 1)
+        return guard(fail(RP_ERR_INVALID, "batch exceeds 2^31 particles"));
+
+    const size_t optin = optinSmem(b->device);
+    b->smemBytes = maxLayout;
+    if (strategy == RP_STRATEGY_FUSED) {
+        if (maxLayout > optin)
+            return guard(fail(RP_ERR_SHARED_MEMORY,
+                              "a rod needs " + std::to_string(maxLayout) +
+                                  " bytes of shared memory; the device allows " + std::to_string(optin) +
+                                  " per block (use RP_STRATEGY_MULTI_KERNEL or a smaller hash table)"));
+        if (rp::plainReserveSmem(std::max<size_t>(maxLayout, 1)) != cudaSuccess) {
+            cudaGetLastError();
+            return guard(fail(RP_ERR_SHARED_MEMORY, "cannot opt into the shared memory the rods need"));
+        }
+    }
+
+    // ---- device buffers ----
+    DArgs& A = b->a;
+    rp_status st;
+#define ALLOC(ptr, T, n) \
+    if ((st = b->alloc(ptr, n)) != RP_OK) return guard(st);
+    DTemplate* dT;
+    DRod* dR;
+    ALLOC(dT, DTemplate, b->tmpls.size());
+    ALLOC(dR, DRod, b->rods.size());
+    A.tmpl = dT;
+    A.rods = dR;
+    float* p_invMass;
+    float4 *p_iI, *p_I, *p_sC, *p_bC, *p_bD;
+    int32_t *p_sP0, *p_sP1, *p_sSeg, *p_bA, *p_bB, *p_order, *p_cs;
+    ALLOC(p_invMass, float, tInvMass.size());
+    ALLOC(p_iI, float4, tInvInertia.size());
+    ALLOC(p_I, float4, tInertia.size());
+    ALLOC(p_sP0, int32_t, tSP0.size());
+    ALLOC(p_sP1, int32_t, tSP1.size());
+    ALLOC(p_sSeg, int32_t, tSSeg.size());
+    ALLOC(p_sC, float4, tSComp.size());
+    ALLOC(p_bA, int32_t, tBA.size());
+    ALLOC(p_bB, int32_t, tBB.size());
+    ALLOC(p_bC, float4, tBComp.size());
+    ALLOC(p_bD, float4, tBRestD.size());
+    ALLOC(p_order, int32_t, tOrder.size());
+    ALLOC(p_cs, int32_t, tColorStart.size());
+    DPrim* p_prims;
+    ALLOC(p_prims, DPrim, prims.size());
+    float *p_cscale, *p_fscale;
+    ALLOC(p_cscale, float, numRods);
+    ALLOC(p_fscale, float, numRods);
+    A.tInvMass = p_invMass;
+    A.tInvInertia = p_iI;
+    A.tInertia = p_I;
+    A.tSP0 = p_sP0;
+    A.tSP1 = p_sP1;
+    A.tSSeg = p_sSeg;
+    A.tSComp = p_sC;
+    A.tBA = p_bA;
+    A.tBB = p_bB;
+    A.tBComp = p_bC;
+    A.tBRestD = p_bD;
+    A.tOrder = p_order;
+    A.tColorStart = p_cs;
+    A.prims = p_prims;
+    A.complianceScale = p_cscale;
+    A.frictionScale = p_fscale;
+    const size_t P = size_t(b->totalP), S = size_t(b->totalS);
+    ALLOC(A.x, float4, P);
+    ALLOC(A.v, float4, P);
+    ALLOC(A.force, float4, P);
+    ALLOC(A.kinVel, float4, P);
+    ALLOC(A.xComp, float4, P);
+    ALLOC(A.q, float4, S);
+    ALLOC(A.omega, float4, S);
+    ALLOC(A.torque, float4, S);
+    if (strategy == RP_STRATEGY_MULTI_KERNEL) {
+        ALLOC(A.gxPrev, float4, P);
+        ALLOC(A.gqPrev, float4, S);
+        ALLOC(A.gLamS, float4, size_t(b->totalSt));
+        ALLOC(A.gLamB, float4, size_t(b->totalB));
+        ALLOC(A.gSlots, rp::DSlot, size_t(b->totalSlots));
+        if (b->anySelf) {
+            ALLOC(A.gCentres, float4, size_t(b->totalSt));
+            ALLOC(A.gSelfInt, int32_t, 4 * size_t(b->totalSt));
+            ALLOC(A.gHash, int32_t, size_t(b->totalHash));
+            ALLOC(A.gPool, rp::DSelf, size_t(b->totalPool));
+        }
+        ALLOC(A.gMisc, int32_t, 4 * size_t(numRods));
+    }
+    ALLOC(A.contactState, uint8_t, size_t(b->totalSlots));
+    ALLOC(A.selfCount, int32_t, numRods);
+    ALLOC(A.selfOverflow, int32_t, numRods);
+    ALLOC(A.selfPairs, int32_t, size_t(b->totalPool));
+    ALLOC(A.rodTime, double, numRods);
+#undef ALLOC
+    A.numRods = numRods;
+    A.numWork = numRods;
+    A.maxPrims = b->maxPrims;
+
+    if ((st = b->upload(dT, b->tmpls)) || (st = b->upload(dR, b->rods)) ||
+        (st = b->upload(p_invMass, tInvMass)) || (st = b->upload(p_iI, tInvInertia)) ||
+        (st = b->upload(p_I, tInertia)) || (st = b->upload(p_sP0, tSP0)) ||
+        (st = b->upload(p_sP1, tSP1)) || (st = b->upload(p_sSeg, tSSeg)) ||
+        (st = b->upload(p_sC, tSComp)) || (st = b->upload(p_bA, tBA)) ||
+        (st = b->upload(p_bB, tBB)) || (st = b->upload(p_bC, tBComp)) ||
+        (st = b->upload(p_bD, tBRestD)) || (st = b->upload(p_order, tOrder)) ||
+        (st = b->upload(p_cs, tColorStart)) || (st = b->upload(p_prims, prims)))
+        return guard(st);
+    const std::vector<float> ones(numRods, 1.0f);
+    if ((st = b->upload(p_cscale, ones)) || (st = b->upload(p_fscale, ones))) return guard(st);
+
+    // ---- initial state: every rod from its descriptor ----
+    {
+        std::vector<float4> hx(P), hv(P), hf(P), hk(P), hq(S), hw(S), ht(S);
+        for (int r = 0; r < numRods; ++r) {
+            const rp_rod_desc* d = rods[r];
+            const DRod& R = b->rods[r];
+            packParticles(d, &hx[R.pOff], &hv[R.pOff], &hf[R.pOff], &hk[R.pOff]);
+            packFrames(d, &hq[R.sOff], &hw[R.sOff], &ht[R.sOff]);
+        }
+        if ((st = b->upload(A.x, hx)) || (st = b->upload(A.v, hv)) || (st = b->upload(A.force, hf)) ||
+            (st = b->upload(A.kinVel, hk)) || (st = b->upload(A.q, hq)) ||
+            (st = b->upload(A.omega, hw)) || (st = b->upload(A.torque, ht)))
+            return guard(st);
+        // the host vectors die here: finish the copies first
+        if (cudaStreamSynchronize(b->stream) != cudaSuccess)
+            return guard(fail(RP_ERR_CUDA, "upload failed"));
+    }
+
+    if (strategy == RP_STRATEGY_BATCHED) {
+        if ((st = buildBatchedPlan(b)) != RP_OK) return guard(st);
+    }
+    *out = b;
+    return RP_OK;
+}
+
+// ---------------------------------------------------------------- batched plan
+
+namespace {
+
+// Team size for a rod of nSt segments: enough threads that each handles about
+// `pairsPerThread` constraints of a colour, rounded to whole warps, 32..256.
+int teamThreads(int nSt, int pairsPerThread) {
+    int t = (nSt / 2 + pairsPerThread - 1) / pairsPerThread;
+    t = (t + 31) / 32 * 32;
+    return std::max(32, std::min(256, t));
+}
+
+rp_status buildBatchedPlan(rp_batch* b) {
+    // Length-sorted work order: longest first, so the tail of the persistent
+    // queue is short rods and the SMs finish together.
+    std::vector<int32_t> order(b->numRods);
+    for (int r = 0; r < b->numRods; ++r) order[r] = r;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        const int nx = b->tmpls[b->rods[x].tmpl].nSt, ny = b->tmpls[b->rods[y].tmpl].nSt;
+        return nx > ny;
+    });
+    const int cta = b->tune.ctaThreads;
+    b->groups.clear();
+    size_t maxSmem = 0;
+    int i = 0;
+    while (i < b->numRods) {
+        const DRod& R0 = b->rods[order[i]];
+        const int team = std::min(cta, teamThreads(b->tmpls[R0.tmpl].nSt, b->tune.pairsPerThread));
+        const int perCta = cta / team;
+        int cnt = 0;
+        size_t smem = 0;
+        while (i + cnt < b->numRods && cnt < perCta) {
+            const DRod& R = b->rods[order[i + cnt]];
+            const DTemplate& T = b->tmpls[R.tmpl];
+            if (std::min(cta, teamThreads(T.nSt, b->tune.pairsPerThread)) != team) break;
+            const rp::RodLayout L =
+                rp::rodLayout(T.nP, T.nS, T.nSt, T.nB, R.numPrims, R.selfCollision, R.hashTableSize,
+                              R.selfCapacity, 1, (b->precision & RP_PRECISION_COMPENSATED) ? 1 : 0);
+            smem += size_t(L.bytes);
+            ++cnt;
+        }
+        b->groups.push_back(i);
+        b->groups.push_back(cnt);
+        b->groups.push_back(team);
+        b->groups.push_back(int32_t(smem));
+        maxSmem = std::max(maxSmem, smem);
+        i += cnt;
+    }
+    b->numGroups = int(b->groups.size() / 4);
+    const size_t optin = optinSmem(b->device);
+    if (maxSmem + 1024 > optin)  // the kernel also has a few bytes of static shared memory
+        return fail(RP_ERR_SHARED_MEMORY, "a rod group needs " + std::to_string(maxSmem) +
+                                              " bytes of shared memory; the device allows " +
+                                              std::to_string(optin));
+    b->batchedSmem = maxSmem;
+    b->batchedThreads = cta;
+    if (rp::batchedReserveSmem(std::max<size_t>(maxSmem, 1)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(RP_ERR_SHARED_MEMORY, "cannot opt into the batched shared memory");
+    }
+    int perSm = 0;
+    if (rp::batchedOccupancy(cta, maxSmem, &perSm) != cudaSuccess || perSm < 1) {
+        cudaGetLastError();
+        return fail(RP_ERR_SHARED_MEMORY, "batched kernel cannot be resident with this group size");
+    }
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+    b->batchedBlocks = std::max(1, std::min(b->numGroups, sms * perSm));
+    if (!b->dWork) {
+        rp_status st;
+        if ((st = b->alloc(b->dWork, b->numRods)) != RP_OK) return st;
+        if ((st = b->alloc(b->dQueue, 2)) != RP_OK) return st;
+    }
+    if (b->dGroups) {
+        cudaFree(b->dGroups);
+        b->owned.erase(std::find(b->owned.begin(), b->owned.end(), static_cast<void*>(b->dGroups)));
+        b->dGroups = nullptr;
+    }
+    rp_status st;
+    if ((st = b->alloc(b->dGroups, b->groups.size())) != RP_OK) return st;
+    if ((st = b->upload(b->dWork, order)) != RP_OK) return st;
+    if ((st = b->upload(b->dGroups, b->groups)) != RP_OK) return st;
+    RP_CUDA(cudaStreamSynchronize(b->stream));
+    b->a.work = b->dWork;
+    return RP_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- stepping
+
+namespace {
+
+void fillStepArgs(rp_batch* b, const rp_step_params* p, DArgs& A) {
+    A.h = p->dt / p->substeps;
+    A.invH2 = 1.0f / (A.h * A.h);
+    A.substeps = p->substeps;
+    A.iterations = p->iterations;
+    A.gx = p->gravity[0];
+    A.gy = p->gravity[1];
+    A.gz = p->gravity[2];
+    A.linDecay = std::exp(-p->linear_damping * A.h);
+    A.angDecay = std::exp(-p->angular_damping * A.h);
+    A.contactInterval = p->contact_interval > 0 ? p->contact_interval : 1;
+    A.dt = p->dt;
+    A.precision = b->precision;
+}
+
+rp_status validateParams(const rp_step_params* p) {
+    if (!p) return fail(RP_ERR_INVALID, "params is NULL");
+    if (!(p->dt > 0) || !std::isfinite(p->dt) || p->substeps < 1 || p->iterations < 0 ||
+        p->substeps > 100000 || p->iterations > 10000)
+        return fail(RP_ERR_INVALID, "params need dt > 0, 1 <= substeps, 0 <= iterations");
+    return RP_OK;
+}
+
+rp_status launchStep(rp_batch* b, const rp_step_params* p) {
+    DArgs A = b->a;
+    fillStepArgs(b, p, A);
+    cudaError_t e;
+    if (b->strategy == RP_STRATEGY_BATCHED) {
+        rp::BatchedPlan plan;
+        plan.groups = b->dGroups;
+        plan.numGroups = b->numGroups;
+        plan.queue = b->dQueue;
+        plan.blocks = b->batchedBlocks;
+        plan.threads = b->batchedThreads;
+        plan.smemBytes = b->batchedSmem;
+        e = rp::launchBatchedStep(A, plan, b->precision, b->stream);
+        b->launches += 2;
+    } else {
+        A.work = nullptr;
+        e = rp::launchPlainStep(A, b->strategy == RP_STRATEGY_MULTI_KERNEL, b->precision,
+                                b->plainThreads, b->smemBytes, b->stream);
+        b->launches += 1;
+    }
+    if (e != cudaSuccess) return fail(RP_ERR_CUDA, std::string("step launch failed: ") + cudaGetErrorString(e));
+    return RP_OK;
+}
+
+rp_status syncBatch(rp_batch* b) {
+    const cudaError_t e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return fail(RP_ERR_CUDA, std::string("stream error: ") + cudaGetErrorString(e));
+    return RP_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- C ABI
+
+extern "C" {
+
+int32_t rp_abi_version(void) { return RP_ABI_VERSION; }
+
+const char* rp_last_error(void) { return g_lastError.c_str(); }
+
+int32_t rp_cuda_available(void) { return deviceUsable(nullptr) ? 1 : 0; }
+
+rp_status rp_device_name(char* out, size_t cap) {
+    if (!out || cap == 0) return fail(RP_ERR_INVALID, "NULL buffer");
+    std::string why;
+    if (!deviceUsable(&why)) {
+        std::snprintf(out, cap, "unknown");
+        return fail(RP_ERR_NO_DEVICE, why);
+    }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return fail(RP_ERR_CUDA, "cudaGetDeviceProperties");
+    std::snprintf(out, cap, "%s (sm_%d%d, %d SMs, %zu KB shared/block opt-in)", prop.name, prop.major,
+                  prop.minor, prop.multiProcessorCount, prop.sharedMemPerBlockOptin / 1024);
+    return RP_OK;
+}
+
+rp_status rp_diagnostic(char* out, size_t cap) {
+    if (!out || cap == 0) return fail(RP_ERR_INVALID, "NULL buffer");
+    std::string why;
+    if (deviceUsable(&why)) why.clear();
+    std::snprintf(out, cap, "%s", why.c_str());
+    return RP_OK;
+}
+
+int32_t rp_max_fused_segments(void) {
+    if (!deviceUsable(nullptr)) return 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const size_t optin = optinSmem(dev);
+    int best = 0;
+    for (int n = 4; n <= 32767; ++n)
+        if (size_t(rp::rodLayout(n + 1, n, n, n - 1, 0, 0, 0, 0).bytes) <= optin) best = n;
+    return best;
+}
+
+rp_status rp_batch_create(const rp_rod_desc* prototype, int32_t numRods, rp_strategy strategy,
+                          const rp_world* world, rp_batch** out) {
+    if (!prototype) return fail(RP_ERR_INVALID, "prototype is NULL");
+    if (numRods < 1) return fail(RP_ERR_INVALID, "num_rods must be >= 1");
+    std::vector<const rp_rod_desc*> rods(numRods, prototype);
+    return createImpl(rods.data(), numRods, world, world ? 1 : 0, nullptr, strategy, out);
+}
+
+rp_status rp_batch_create_mixed(const rp_rod_desc* const* rods, int32_t numRods, const rp_world* worlds,
+                                int32_t numWorlds, const int32_t* worldOfRod, rp_strategy strategy,
+                                rp_batch** out) {
+    if (!rods) return fail(RP_ERR_INVALID, "rods is NULL");
+    return createImpl(rods, numRods, worlds, numWorlds, worldOfRod, strategy, out);
+}
+
+void rp_batch_destroy(rp_batch* b) {
+    if (b) cudaStreamSynchronize(b->stream);
+    delete b;
+}
+
+rp_status rp_batch_step(rp_batch* b, const rp_step_params* p) {
+    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
+    rp_status st = validateParams(p);
+    if (st != RP_OK) return st;
+    return launchStep(b, p);
+}
+
+rp_status rp_batch_step_many(rp_batch* b, const rp_step_params* p, int32_t steps) {
+    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
+    rp_status st = validateParams(p);
+    if (st != RP_OK) return st;
+    if (steps < 0) return fail(RP_ERR_INVALID, "steps < 0");
+    if (steps == 0) return RP_OK;
+    if (!b->useGraph) {
+        for (int s = 0; s < steps; ++s)
+            if ((st = launchStep(b, p)) != RP_OK) return st;
+        return RP_OK;
+    }
+    const bool same = b->graphExec && b->graphSteps == steps && b->graphPrecision == b->precision &&
+                      std::memcmp(&b->graphParams, p, sizeof(rp_step_params)) == 0;
+    if (!same) {
+        if (b->graphExec) {
+            cudaGraphExecDestroy(b->graphExec);
+            b->graphExec = nullptr;
+        }
+        cudaGraph_t graph = nullptr;
+        RP_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        const long long before = b->launches;
+        for (int s = 0; s < steps; ++s) {
+            st = launchStep(b, p);
+            if (st != RP_OK) {
+                cudaStreamEndCapture(b->stream, &graph);
+                if (graph) cudaGraphDestroy(graph);
+                return st;
+            }
+        }
+        b->launches = before;
+        RP_CUDA(cudaStreamEndCapture(b->stream, &graph));
+        const cudaError_t e = cudaGraphInstantiate(&b->graphExec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return fail(RP_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+        b->graphSteps = steps;
+        b->graphParams = *p;
+        b->graphPrecision = b->precision;
+    }
+    RP_CUDA(cudaGraphLaunch(b->graphExec, b->stream));
+    b->launches += (b->strategy == RP_STRATEGY_BATCHED ? 2 : 1) * int64_t(steps);
+    return RP_OK;
+}
+
+rp_status rp_batch_synchronize(rp_batch* b) {
+    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
+    return syncBatch(b);
+}
+
+rp_status rp_batch_set_stream(rp_batch* b, void* stream) {
+    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
+    rp_status st = syncBatch(b);
+    if (st != RP_OK) return st;
+    if (b->ownStream && b->stream) cudaStreamDestroy(b->stream);
+    if (stream) {
+        b->stream = static_cast<cudaStream_t>(stream);
+        b->ownStream = false;
+    } else {
+        RP_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+        b->ownStream = true;
+    }
+    if (b->graphExec) {
+        cudaGraphExecDestroy(b->graphExec);
+        b->graphExec = nullptr;
+    }
+    return RP_OK;
+}
+
+rp_status rp_batch_set_precision(rp_batch* b, int32_t flags) {
+    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
+    if (flags & ~7) return fail(RP_ERR_INVALID, "unknown precision flag");
+    if ((flags & RP_PRECISION_COMPENSATED) != (b->precision & RP_PRECISION_COMPENSATED)) {
+        // entering or leaving compensated mode: the compensation starts at zero
+        RP_CUDA(cudaMemsetAsync(b->a.xComp, 0, size_t(b->totalP) * sizeof(float4), b->stream));
+        b->precision = flags;
+        // the batched layout keeps the compensation in shared memory
+        if (b->strategy == RP_STRATEGY_BATCHED) {
+            rp_status st = buildBatchedPlan(b);
+            if (st != RP_OK) return st;
+        }
+        if (b->graphExec) {
+            cudaGraphExecDestroy(b->graphExec);
+            b->graphExec = nullptr;
+        }
+    }
+    b->precision = flags;
+    return RP_OK;
+}
+
+rp_status rp_batch_set_graph(rp_batch* b, int32_t enabled) {
+    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
+    b->useGraph = enabled != 0;
+    return RP_OK;
+}
+
+rp_status rp_batch_download(rp_batch* b, int32_t rod, rp_rod_desc* out) {
+    if (!b || !out) return fail(RP_ERR_INVALID, "batch or out is NULL");
+    if (rod < 0 || rod >= b->numRods) return fail(RP_ERR_INVALID, "rod index out of range");
+    if (!sameTopology(b, rod, out) || !out->x || !out->q)
+        return fail(RP_ERR_INVALID, "out does not have the rod's topology");
+    const DRod& R = b->rods[rod];
+    const int nP = b->tmplNP[rod], nS = b->tmplNS[rod];
+    std::vector<float4> x(nP), v(nP), c(nP), q(nS), w(nS);
+    RP_CUDA(cudaMemcpyAsync(x.data(), b->a.x + R.pOff, nP * sizeof(float4), cudaMemcpyDeviceToHost, b->stream));
+    RP_CUDA(cudaMemcpyAsync(v.data(), b->a.v + R.pOff, nP * sizeof(float4), cudaMemcpyDeviceToHost, b->stream));
+    RP_CUDA(cudaMemcpyAsync(c.data(), b->a.xComp + R.pOff, nP * sizeof(float4), cudaMemcpyDeviceToHost, b->stream));
+    RP_CUDA(cudaMemcpyAsync(q.data(), b->a.q + R.sOff, nS * sizeof(float4), cudaMemcpyDeviceToHost, b->stream));
+    RP_CUDA(cudaMemcpyAsync(w.data(), b->a.omega + R.sOff, nS * sizeof(float4), cudaMemcpyDeviceToHost, b->stream));
+    rp_status st = syncBatch(b);
+    if (st != RP_OK) return st;
+    const bool comp = (b->precision & RP_PRECISION_COMPENSATED) != 0;
+    for (int i = 0; i < nP; ++i) {
+        out->x[3 * i] = double(x[i].x) - (comp ? double(c[i].x) : 0.0);
+        out->x[3 * i + 1] = double(x[i].y) - (comp ? double(c[i].y) : 0.0);
+        out->x[3 * i + 2] = double(x[i].z) - (comp ? double(c[i].z) : 0.0);
+        if (out->v) {
+            out->v[3 * i] = v[i].x;
+            out->v[3 * i + 1] = v[i].y;
+            out->v[3 * i + 2] = v[i].z;
+        }
+    }
+    for (int j = 0; j < nS; ++j) {
+        out->q[4 * j] = q[j].x;
+        out->q[4 * j + 1] = q[j].y;
+        out->q[4 * j + 2] = q[j].z;
+        out->q[4 * j + 3] = q[j].w;
+        if (out->omega) {
+            out->omega[3 * j] = w[j].x;
+            out->omega[3 * j + 1] = w[j].y;
+            out->omega[3 * j + 2] = w[j].z;
+        }
+    }
+    return RP_OK;
+}
+
+rp_status rp_batch_download_positions(rp_batch* b, float* out, int64_t cap) {
+    if (!b || !out) return fail(RP_ERR_INVALID, "batch or out is NULL");
+    const size_t P = size_t(b->totalP);
+    if (cap < int64_t(3 * P)) return fail(RP_ERR_INVALID, "capacity below 3 x total particles");
+    std::vector<float4> x(P), c;
+    RP_CUDA(cudaMemcpyAsync(x.data(), b->a.x, P * sizeof(float4), cudaMemcpyDeviceToHost, b->stream));
+    const bool comp = (b->precision & RP_PRECISION_COMPENSATED) != 0;
+    if (comp) {
+        c.resize(P);
+        RP_CUDA(cudaMemcpyAsync(c.data(), b->a.xComp, P * sizeof(float4), cudaMemcpyDeviceToHost, b->stream));
+    }
+    rp_status st = syncBatch(b);
+    if (st != RP_OK) return st;
+    for (size_t i = 0; i < P; ++i) {
+        out[3 * i] = comp ? float(double(x[i].x) - double(c[i].x)) : x[i].x;
+        out[3 * i + 1] = comp ? float(double(x[i].y) - double(c[i].y)) : x[i].y;
+        out[3 * i + 2] = comp ? float(double(x[i].z) - double(c[i].z)) : x[i].z;
+    }
+    return RP_OK;
+}
+
+rp_status rp_batch_download_frames(rp_batch* b, float* out, int64_t cap) {
+    if (!b || !out) return fail(RP_ERR_INVALID, "batch or out is NULL");
+    const size_t S = size_t(b->totalS);
+    if (cap < int64_t(4 * S)) return fail(RP_ERR_INVALID, "capacity below 4 x total frames");
+    std::vector<float4> q(S);
+    RP_CUDA(cudaMemcpyAsync(q.data(), b->a.q, S * sizeof(float4), cudaMemcpyDeviceToHost, b->stream));
+    rp_status st = syncBatch(b);
+    if (st != RP_OK) return st;
+    std::memcpy(out, q.data(), S * sizeof(float4));
+    return RP_OK;
+}
+
+static rp_status setLoadsImpl(rp_batch* b, int rod, const rp_rod_desc* s) {
+    const DRod& R = b->rods[rod];
+    const int nP = b->tmplNP[rod], nS = b->tmplNS[rod];
+    std::vector<float4> f(nP), k(nP), t(nS), q(nS);
+    packParticles(s, nullptr, nullptr, f.data(), k.data());
+    packFrames(s, q.data(), nullptr, t.data());
+    RP_CUDA(cudaMemcpyAsync(b->a.force + R.pOff, f.data(), nP * sizeof(float4), cudaMemcpyHostToDevice, b->stream));
+    RP_CUDA(cudaMemcpyAsync(b->a.kinVel + R.pOff, k.data(), nP * sizeof(float4), cudaMemcpyHostToDevice, b->stream));
+    RP_CUDA(cudaMemcpyAsync(b->a.torque + R.sOff, t.data(), nS * sizeof(float4), cudaMemcpyHostToDevice, b->stream));
+    // fixed frames (zero inertia) take their orientation from the source:
+    // how an end is driven, e.g. twisted (gpu_batch.cpp:386-389)
+    const std::vector<char>& fixed = b->fixedFrame[R.tmpl];
+    for (int j = 0; j < nS; ++j)
+        if (fixed[j])
+            RP_CUDA(cudaMemcpyAsync(b->a.q + R.sOff + j, &q[j], sizeof(float4), cudaMemcpyHostToDevice, b->stream));
+    return syncBatch(b);
+}
+
+rp_status rp_batch_set_loads(rp_batch* b, int32_t rod, const rp_rod_desc* s) {
+    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
+    if (rod < 0 || rod >= b->numRods) return fail(RP_ERR_INVALID, "rod index out of range");
+    if (!sameTopology(b, rod, s) || !s->q) return fail(RP_ERR_INVALID, "source does not have the rod's topology");
+    return setLoadsImpl(b, rod, s);
+}
+
+static rp_status uploadRodImpl(rp_batch* b, int rod, const rp_rod_desc* s) {
+    const DRod& R = b->rods[rod];
+    const int nP = b->tmplNP[rod], nS = b->tmplNS[rod];
+    std::vector<float4> x(nP), v(nP), q(nS), w(nS), z(nP, make_float4(0, 0, 0, 0));
+    packParticles(s, x.data(), v.data(), nullptr, nullptr);
+    packFrames(s, q.data(), w.data(), nullptr);
+    RP_CUDA(cudaMemcpyAsync(b->a.x + R.pOff, x.data(), nP * sizeof(float4), cudaMemcpyHostToDevice, b->stream));
+    RP_CUDA(cudaMemcpyAsync(b->a.v + R.pOff, v.data(), nP * sizeof(float4), cudaMemcpyHostToDevice, b->stream));
+    RP_CUDA(cudaMemcpyAsync(b->a.xComp + R.pOff, z.data(), nP * sizeof(float4), cudaMemcpyHostToDevice, b->stream));
+    RP_CUDA(cudaMemcpyAsync(b->a.q + R.sOff, q.data(), nS * sizeof(float4), cudaMemcpyHostToDevice, b->stream));
+    RP_CUDA(cudaMemcpyAsync(b->a.omega + R.sOff, w.data(), nS * sizeof(float4), cudaMemcpyHostToDevice, b->stream));
+    return setLoadsImpl(b, rod, s);
+}
+
+rp_status rp_batch_upload_rod(rp_batch* b, int32_t rod, const rp_rod_desc* s) {
+    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
+    if (rod < 0 || rod >= b->numRods) return fail(RP_ERR_INVALID, "rod index out of range");
+    if (!sameTopology(b, rod, s) || !s->x || !s->q)
+        return fail(RP_ERR_INVALID, "source does not have the rod's topology");
+    return uploadRodImpl(b, rod, s);
+}
+
+rp_status rp_batch_upload(rp_batch* b, const rp_rod_desc* s) {
+    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
+    for (int r = 0; r < b->numRods; ++r) {
+        if (!sameTopology(b, r, s) || !s->x || !s->q)
+            return fail(RP_ERR_INVALID, "source does not have rod " + std::to_string(r) + "'s topology");
+    }
+    const size_t P = size_t(b->totalP), S = size_t(b->totalS);
+    std::vector<float4> hx(P), hv(P), hf(P), hk(P), hq(S), hw(S), ht(S);
+    for (int r = 0; r < b->numRods; ++r) {
+        const DRod& R = b->rods[r];
+        packParticles(s, &hx[R.pOff], &hv[R.pOff], &hf[R.pOff], &hk[R.pOff]);
+        packFrames(s, &hq[R.sOff], &hw[R.sOff], &ht[R.sOff]);
+    }
+    rp_status st;
+    if ((st = b->upload(b->a.x, hx)) || (st = b->upload(b->a.v, hv)) || (st = b->upload(b->a.force, hf)) ||
+        (st = b->upload(b->a.kinVel, hk)) || (st = b->upload(b->a.q, hq)) || (st = b->upload(b->a.omega, hw)) ||
+        (st = b->upload(b->a.torque, ht)))
+        return st;
+    RP_CUDA(cudaMemsetAsync(b->a.xComp, 0, P * sizeof(float4), b->stream));
+    return syncBatch(b);
+}
+
+rp_status rp_batch_set_kinematic_velocities(rp_batch* b, const float* xyz, int64_t count) {
+    if (!b || !xyz) return fail(RP_ERR_INVALID, "batch or data is NULL");
+    if (count != b->totalP) return fail(RP_ERR_INVALID, "count must equal the total particle count");
+    std::vector<float4> k(static_cast<size_t>(count));
+    for (int64_t i = 0; i < count; ++i) k[i] = make_float4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], 0.0f);
+    rp_status st = b->upload(b->a.kinVel, k);
+    if (st != RP_OK) return st;
+    return syncBatch(b);
+}
+
+rp_status rp_batch_set_material_scales(rp_batch* b, const float* youngs, const float* friction, int32_t n) {
+    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
+    if ((youngs || friction) && n != b->numRods) return fail(RP_ERR_INVALID, "n must equal num_rods");
+    if (youngs) {
+        std::vector<float> c(n);
+        for (int r = 0; r < n; ++r) {
+            if (!(youngs[r] > 0)) return fail(RP_ERR_INVALID, "youngs_scale must be positive");
+            c[r] = 1.0f / youngs[r];
+        }
+        rp_status st = b->upload(const_cast<float*>(b->a.complianceScale), c);
+        if (st != RP_OK) return st;
+    }
+    if (friction) {
+        std::vector<float> f(friction, friction + n);
+        rp_status st = b->upload(const_cast<float*>(b->a.frictionScale), f);
+        if (st != RP_OK) return st;
+    }
+    return syncBatch(b);
+}
+
+rp_status rp_batch_set_drives(rp_batch* b, const rp_drive* drives, int32_t n) {
+    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
+    if (!drives) {
+        b->a.drives = nullptr;
+        return RP_OK;
+    }
+    if (n != b->numRods) return fail(RP_ERR_INVALID, "n must equal num_rods");
+    std::vector<rp::DDrive> d(n);
+    for (int r = 0; r < n; ++r) {
+        d[r].particle = drives[r].particle;
+        if (d[r].particle >= b->tmplNP[r]) return fail(RP_ERR_INVALID, "drive particle out of range");
+        d[r].ax = drives[r].axis[0];
+        d[r].ay = drives[r].axis[1];
+        d[r].az = drives[r].axis[2];
+        d[r].amplitude = drives[r].amplitude;
+        d[r].omega = float(2.0 * 3.14159265358979323846 * double(drives[r].frequency));
+        d[r].phase = drives[r].phase;
+    }
+    rp::DDrive* dd = const_cast<rp::DDrive*>(b->a.drives);
+    if (!dd) {
+        rp_status st = b->alloc(dd, size_t(n));
+        if (st != RP_OK) return st;
+    }
+    rp_status st = b->upload(dd, d);
+    if (st != RP_OK) return st;
+    b->a.drives = dd;
+    if (b->graphExec) {
+        cudaGraphExecDestroy(b->graphExec);
+        b->graphExec = nullptr;
+    }
+    return syncBatch(b);
+}
+
+rp_status rp_batch_set_time(rp_batch* b, double t) {
+    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
+    std::vector<double> tt(b->numRods, t);
+    rp_status st = b->upload(b->a.rodTime, tt);
+    if (st != RP_OK) return st;
+    return syncBatch(b);
+}
+
+rp_status rp_batch_read_state_async(rp_batch* b, int32_t what, void* dst, int64_t bytes) {
+    if (!b || !dst) return fail(RP_ERR_INVALID, "batch or dst is NULL");
+    const void* src = nullptr;
+    int64_t size = 0;
+    switch (what) {
+        case RP_STATE_POSITIONS: src = b->a.x; size = b->totalP * 16; break;
+        case RP_STATE_FRAMES: src = b->a.q; size = b->totalS * 16; break;
+        case RP_STATE_CONTACTS: src = b->a.contactState; size = b->totalSlots; break;
+        default: return fail(RP_ERR_INVALID, "unknown state array for reading");
+    }
+    if (bytes != size) return fail(RP_ERR_INVALID, "bytes must be " + std::to_string(size));
+    if (size > 0) RP_CUDA(cudaMemcpyAsync(dst, src, size_t(size), cudaMemcpyDeviceToHost, b->stream));
+    return RP_OK;
+}
+
+rp_status rp_batch_write_state_async(rp_batch* b, int32_t what, const void* src, int64_t bytes) {
+    if (!b || !src) return fail(RP_ERR_INVALID, "batch or src is NULL");
+    if (what != RP_STATE_KINEMATIC) return fail(RP_ERR_INVALID, "only RP_STATE_KINEMATIC is writable");
+    const int64_t size = b->totalP * 16;
+    if (bytes != size) return fail(RP_ERR_INVALID, "bytes must be " + std::to_string(size));
+    RP_CUDA(cudaMemcpyAsync(b->a.kinVel, src, size_t(size), cudaMemcpyHostToDevice, b->stream));
+    return RP_OK;
+}
+
+rp_status rp_batch_read_contact_states(rp_batch* b, uint8_t* out, int64_t cap, int64_t* count) {
+    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
+    if (count) *count = b->totalSlots;
+    if (!out) return RP_OK;
+    if (cap < b->totalSlots) return fail(RP_ERR_INVALID, "capacity below the slot count");
+    if (b->totalSlots > 0)
+        RP_CUDA(cudaMemcpyAsync(out, b->a.contactState, size_t(b->totalSlots), cudaMemcpyDeviceToHost, b->stream));
+    return syncBatch(b);
+}
+
+rp_status rp_batch_read_self_contacts(rp_batch* b, int32_t rod, int32_t* pairs, int32_t cap, int32_t* count) {
+    if (!b || !count) return fail(RP_ERR_INVALID, "batch or count is NULL");
+    if (rod < 0 || rod >= b->numRods) return fail(RP_ERR_INVALID, "rod index out of range");
+    const DRod& R = b->rods[rod];
+    *count = 0;
+    if (!R.selfCollision) return RP_OK;
+    int32_t live = 0;
+    RP_CUDA(cudaMemcpyAsync(&live, b->a.selfCount + rod, sizeof(int32_t), cudaMemcpyDeviceToHost, b->stream));
+    rp_status st = syncBatch(b);
+    if (st != RP_OK) return st;
+    *count = live;
+    if (!pairs || live == 0) return RP_OK;
+    if (cap < live) return fail(RP_ERR_INVALID, "capacity below the pair count");
+    std::vector<int32_t> enc(live);
+    RP_CUDA(cudaMemcpyAsync(enc.data(), b->a.selfPairs + R.poolOff, live * sizeof(int32_t),
+                            cudaMemcpyDeviceToHost, b->stream));
+    if ((st = syncBatch(b)) != RP_OK) return st;
+    for (int c = 0; c < live; ++c) {
+        pairs[2 * c] = enc[c] >> 16;
+        pairs[2 * c + 1] = enc[c] & 0xffff;
+    }
+    return RP_OK;
+}
+
+rp_status rp_batch_arm_hold_observer(rp_batch* b, const int32_t* particle, int32_t n, int32_t interval,
+                                     double tolerance) {
+    if (!b || !particle) return fail(RP_ERR_INVALID, "batch or particle is NULL");
+    if (n != b->numRods || interval < 1) return fail(RP_ERR_INVALID, "n must equal num_rods, interval >= 1");
+    const size_t P = size_t(b->totalP);
+    std::vector<float4> x(P), c(P);
+    RP_CUDA(cudaMemcpyAsync(x.data(), b->a.x, P * sizeof(float4), cudaMemcpyDeviceToHost, b->stream));
+    RP_CUDA(cudaMemcpyAsync(c.data(), b->a.xComp, P * sizeof(float4), cudaMemcpyDeviceToHost, b->stream));
+    rp_status st = syncBatch(b);
+    if (st != RP_OK) return st;
+    const bool comp = (b->precision & RP_PRECISION_COMPENSATED) != 0;
+    std::vector<rp::DHold> h(n);
+    for (int r = 0; r < n; ++r) {
+        h[r].particle = particle[r];
+        if (particle[r] >= b->tmplNP[r]) return fail(RP_ERR_INVALID, "observer particle out of range");
+        h[r].steps = 0;
+        h[r].maxRise = 0.0;
+        h[r].startZ = 0.0;
+        if (particle[r] >= 0) {
+            const size_t i = size_t(b->rods[r].pOff) + particle[r];
+            h[r].startZ = double(x[i].z) - (comp ? double(c[i].z) : 0.0);
+        }
+    }
+    if (!b->a.hold) {
+        rp::DHold* dh = nullptr;
+        if ((st = b->alloc(dh, size_t(n))) != RP_OK) return st;
+        b->a.hold = dh;
+    }
+    if ((st = b->upload(b->a.hold, h)) != RP_OK) return st;
+    b->a.holdInterval = interval;
+    b->holdInterval = interval;
+    b->holdTolerance = tolerance;
+    b->holdArmed = true;
+    if (b->graphExec) {
+        cudaGraphExecDestroy(b->graphExec);
+        b->graphExec = nullptr;
+    }
+    return syncBatch(b);
+}
+
+rp_status rp_batch_read_hold_verdicts(rp_batch* b, double* maxRise, uint8_t* held, uint8_t* nearBoundary,
+                                      int32_t n) {
+    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
+    if (!b->holdArmed) return fail(RP_ERR_INVALID, "hold observer not armed");
+    if (n != b->numRods) return fail(RP_ERR_INVALID, "n must equal num_rods");
+    // final sample of the run (the reference samples at the last step too,
+    // application_cases.cpp:59)
+    const cudaError_t e = rp::launchObserve(b->a, (b->precision & RP_PRECISION_COMPENSATED) != 0, b->stream);
+    if (e != cudaSuccess) return fail(RP_ERR_CUDA, cudaGetErrorString(e));
+    b->launches += 1;
+    std::vector<rp::DHold> h(n);
+    RP_CUDA(cudaMemcpyAsync(h.data(), b->a.hold, n * sizeof(rp::DHold), cudaMemcpyDeviceToHost, b->stream));
+    rp_status st = syncBatch(b);
+    if (st != RP_OK) return st;
+    for (int r = 0; r < n; ++r) {
+        if (maxRise) maxRise[r] = h[r].maxRise;
+        if (held) held[r] = h[r].maxRise <= b->holdTolerance ? 1 : 0;
+        if (nearBoundary) {
+            // within a few float spacings of the threshold at the observed height
+            const float zf = float(h[r].startZ + b->holdTolerance);
+            const double spacing = double(std::nextafter(std::fabs(zf), 2.0f * std::fabs(zf) + 1.0f)) -
+                                   double(std::fabs(zf));
+            nearBoundary[r] = std::fabs(h[r].maxRise - b->holdTolerance) <= 4.0 * spacing ? 1 : 0;
+        }
+    }
+    return RP_OK;
+}
+
+int32_t rp_batch_num_rods(const rp_batch* b) { return b ? b->numRods : 0; }
+int32_t rp_batch_num_segments(const rp_batch* b, int32_t rod) {
+    if (!b || rod < 0 || rod >= b->numRods) return 0;
+    return b->tmpls[b->rods[rod].tmpl].nSt;
+}
+int32_t rp_batch_num_particles(const rp_batch* b, int32_t rod) {
+    if (!b || rod < 0 || rod >= b->numRods) return 0;
+    return b->tmplNP[rod];
+}
+int64_t rp_batch_particle_offset(const rp_batch* b, int32_t rod) {
+    if (!b || rod < 0 || rod >= b->numRods) return -1;
+    return b->rods[rod].pOff;
+}
+int32_t rp_batch_num_frames(const rp_batch* b, int32_t rod) {
+    if (!b || rod < 0 || rod >= b->numRods) return 0;
+    return b->tmplNS[rod];
+}
+int64_t rp_batch_frame_offset(const rp_batch* b, int32_t rod) {
+    if (!b || rod < 0 || rod >= b->numRods) return -1;
+    return b->rods[rod].sOff;
+}
+int32_t rp_batch_strategy(const rp_batch* b) { return b ? int32_t(b->strategy) : -1; }
+int32_t rp_batch_stretch_colors(const rp_batch* b) { return b ? b->sColorsMax : 0; }
+int32_t rp_batch_bend_colors(const rp_batch* b) { return b ? b->bColorsMax : 0; }
+size_t rp_batch_shared_bytes_per_block(const rp_batch* b) {
+    if (!b) return 0;
+    return b->strategy == RP_STRATEGY_BATCHED ? b->batchedSmem
+           : b->strategy == RP_STRATEGY_FUSED ? b->smemBytes
+                                              : 0;
+}
+int32_t rp_batch_launches_per_step(const rp_batch* b, const rp_step_params*) {
+    if (!b) return 0;
+    return b->strategy == RP_STRATEGY_BATCHED ? 2 : 1;
+}
+int64_t rp_batch_self_contact_overflow(rp_batch* b) {
+    if (!b || !b->anySelf) return 0;
+    std::vector<int32_t> o(b->numRods);
+    if (cudaMemcpyAsync(o.data(), b->a.selfOverflow, o.size() * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                        b->stream) != cudaSuccess ||
+        cudaStreamSynchronize(b->stream) != cudaSuccess) {
+        fail(RP_ERR_CUDA, "overflow read failed");
+        return -1;
+    }
+    int64_t t = 0;
+    for (int32_t v : o) t += v;
+    return t;
+}
+int64_t rp_batch_kernel_launches(const rp_batch* b) { return b ? b->launches : 0; }
+
+}  // extern "C"

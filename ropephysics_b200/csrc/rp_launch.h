@@ -1,0 +1,34 @@
+// rp_launch.h -- host-callable kernel launchers (implemented in the .cu files).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "rp_internal.h"
+
+namespace rp {
+
+// Plain one-rod-per-CTA step (RP_STRATEGY_FUSED with gmem = 0,
+// RP_STRATEGY_MULTI_KERNEL with gmem = 1).
+cudaError_t launchPlainStep(const DArgs& a, int gmem, int precision, int threads,
+                            size_t smemBytes, cudaStream_t stream);
+// Opt the plain kernels into `bytes` of dynamic shared memory (up to 227 KB).
+cudaError_t plainReserveSmem(size_t bytes);
+
+// Persistent batched step (RP_STRATEGY_BATCHED).
+struct BatchedPlan {
+    const int32_t* groups;  // device: per group {firstWork, count, teamThreads, smemPerRod}
+    int32_t numGroups;
+    int32_t* queue;         // device work counter (reset by the launcher)
+    int32_t blocks;         // persistent grid size
+    int32_t threads;        // CTA size
+    size_t smemBytes;       // dynamic shared memory per CTA
+};
+cudaError_t launchBatchedStep(const DArgs& a, const BatchedPlan& plan, int precision,
+                              cudaStream_t stream);
+cudaError_t batchedReserveSmem(size_t bytes);
+cudaError_t batchedOccupancy(int threads, size_t smemBytes, int* blocksPerSm);
+
+// One hold observation of every armed rod (the final sample of a run).
+cudaError_t launchObserve(const DArgs& a, int compensated, cudaStream_t stream);
+
+}  // namespace rp

@@ -1,0 +1,278 @@
+// rp_math.cuh -- FP32 vector/quaternion/matrix algebra for the rod kernels.
+//
+// The formulas are those of the reference's shared math (src/core/math3.h and
+// src/core/geometry.h): the algorithm, and with it the order of every
+// floating-point operation, must be the same for the GPU results to agree
+// with the reference's FP32 GPU path to rounding. In particular
+// "vector / scalar" is "vector * (1 / scalar)" (math3.h:75-78), and
+// expression trees are kept in the reference's association so that nvcc's
+// FMA contraction makes the same choices. The code is written for this
+// library (register-friendly structs, no templates on the scalar).
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace rp {
+
+struct V3 {
+    float x, y, z;
+};
+struct Q4 {
+    float w, x, y, z;
+};
+struct M3 {
+    float m[3][3];
+};
+
+__device__ __forceinline__ V3 v3(float x, float y, float z) { return V3{x, y, z}; }
+__device__ __forceinline__ V3 v3(float4 a) { return V3{a.x, a.y, a.z}; }
+__device__ __forceinline__ float4 f4(V3 a) { return make_float4(a.x, a.y, a.z, 0.0f); }
+__device__ __forceinline__ Q4 q4(float4 a) { return Q4{a.x, a.y, a.z, a.w}; }
+__device__ __forceinline__ float4 f4(Q4 q) { return make_float4(q.w, q.x, q.y, q.z); }
+
+__device__ __forceinline__ V3 operator+(V3 a, V3 b) { return V3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ V3 operator-(V3 a, V3 b) { return V3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ V3 operator-(V3 a) { return V3{-a.x, -a.y, -a.z}; }
+__device__ __forceinline__ V3 operator*(V3 a, float s) { return V3{a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ V3 divs(V3 a, float s) { return a * (1.0f / s); }
+__device__ __forceinline__ float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ V3 cross(V3 a, V3 b) {
+    return V3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ float norm2(V3 a) { return dot(a, a); }
+__device__ __forceinline__ float norm(V3 a) { return sqrtf(dot(a, a)); }
+__device__ __forceinline__ V3 cwise(V3 a, V3 b) { return V3{a.x * b.x, a.y * b.y, a.z * b.z}; }
+
+__device__ __forceinline__ M3 mzero() {
+    M3 r;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) r.m[i][j] = 0.0f;
+    return r;
+}
+__device__ __forceinline__ M3 midentity(float s) {
+    M3 r = mzero();
+    r.m[0][0] = r.m[1][1] = r.m[2][2] = s;
+    return r;
+}
+__device__ __forceinline__ M3 mskew(V3 v) {
+    M3 r = mzero();
+    r.m[0][1] = -v.z;
+    r.m[0][2] = v.y;
+    r.m[1][0] = v.z;
+    r.m[1][2] = -v.x;
+    r.m[2][0] = -v.y;
+    r.m[2][1] = v.x;
+    return r;
+}
+__device__ __forceinline__ M3 madd(const M3& A, const M3& B) {
+    M3 r;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) r.m[i][j] = A.m[i][j] + B.m[i][j];
+    return r;
+}
+__device__ __forceinline__ M3 mscale(const M3& A, float s) {
+    M3 r;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) r.m[i][j] = A.m[i][j] * s;
+    return r;
+}
+// A diag(d) A^T
+__device__ __forceinline__ M3 sandwichDiag(const M3& A, V3 d) {
+    M3 r;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            r.m[i][j] = A.m[i][0] * d.x * A.m[j][0] + A.m[i][1] * d.y * A.m[j][1] +
+                        A.m[i][2] * d.z * A.m[j][2];
+    return r;
+}
+// Symmetric positive-definite 3x3 solve by Cholesky; false if not SPD.
+__device__ __forceinline__ bool solveSPD3(const M3& A, V3 b, V3& y) {
+    float l00 = A.m[0][0];
+    if (l00 <= 0.0f) return false;
+    l00 = sqrtf(l00);
+    const float l10 = A.m[1][0] / l00;
+    const float l20 = A.m[2][0] / l00;
+    float l11 = A.m[1][1] - l10 * l10;
+    if (l11 <= 0.0f) return false;
+    l11 = sqrtf(l11);
+    const float l21 = (A.m[2][1] - l20 * l10) / l11;
+    float l22 = A.m[2][2] - l20 * l20 - l21 * l21;
+    if (l22 <= 0.0f) return false;
+    l22 = sqrtf(l22);
+    const float z0 = b.x / l00;
+    const float z1 = (b.y - l10 * z0) / l11;
+    const float z2 = (b.z - l20 * z0 - l21 * z1) / l22;
+    y.z = z2 / l22;
+    y.y = (z1 - l21 * y.z) / l11;
+    y.x = (z0 - l10 * y.y - l20 * y.z) / l00;
+    return true;
+}
+
+__device__ __forceinline__ V3 im(Q4 q) { return V3{q.x, q.y, q.z}; }
+__device__ __forceinline__ Q4 qmake(float w, V3 v) { return Q4{w, v.x, v.y, v.z}; }
+// Hamilton product: (aw bw - av.bv, aw bv + bw av + av x bv)
+__device__ __forceinline__ Q4 qmul(Q4 a, Q4 b) {
+    const V3 av = im(a), bv = im(b);
+    return qmake(a.w * b.w - dot(av, bv), bv * a.w + av * b.w + cross(av, bv));
+}
+__device__ __forceinline__ Q4 conj(Q4 q) { return Q4{q.w, -q.x, -q.y, -q.z}; }
+__device__ __forceinline__ Q4 qadd(Q4 a, Q4 b) {
+    return Q4{a.w + b.w, a.x + b.x, a.y + b.y, a.z + b.z};
+}
+__device__ __forceinline__ Q4 qscale(Q4 q, float s) { return Q4{q.w * s, q.x * s, q.y * s, q.z * s}; }
+__device__ __forceinline__ float qdot(Q4 a, Q4 b) {
+    return a.w * b.w + a.x * b.x + a.y * b.y + a.z * b.z;
+}
+__device__ __forceinline__ Q4 qnormalize(Q4 q) {
+    const float n = sqrtf(qdot(q, q));
+    return qscale(q, 1.0f / n);
+}
+// body -> world
+__device__ __forceinline__ V3 rotate(Q4 q, V3 v) {
+    const V3 u = im(q);
+    const V3 t = cross(u, v) * 2.0f;
+    return v + t * q.w + cross(u, t);
+}
+__device__ __forceinline__ V3 rotateInv(Q4 q, V3 v) { return rotate(conj(q), v); }
+// q <- normalize(q * (1, theta / 2)), theta a body-frame rotation vector
+__device__ __forceinline__ Q4 applyBodyDelta(Q4 q, V3 theta) {
+    return qnormalize(qmul(q, qmake(1.0f, theta * 0.5f)));
+}
+// Representative on the same hemisphere as the identity.
+__device__ __forceinline__ Q4 sameHemisphereId(Q4 q) {
+    return qdot(q, Q4{1.0f, 0.0f, 0.0f, 0.0f}) < 0.0f ? qscale(q, -1.0f) : q;
+}
+
+// ---------------------------------------------------------------- geometry
+
+__device__ __forceinline__ float clamp01(float v) { return v < 0.0f ? 0.0f : (v > 1.0f ? 1.0f : v); }
+__device__ __forceinline__ float absT(float v) { return v < 0.0f ? -v : v; }
+__device__ __forceinline__ float clampT(float v, float lo, float hi) {
+    return v < lo ? lo : (v > hi ? hi : v);
+}
+
+__device__ __forceinline__ float distanceToSphereLike(V3 centre, float radius, V3 p, V3& n) {
+    const V3 d = p - centre;
+    const float len = norm(d);
+    n = len > 1e-12f ? divs(d, len) : V3{0.0f, 0.0f, 1.0f};
+    return len - radius;
+}
+
+// Signed distance to a primitive's surface and its outward normal.
+struct PrimF {
+    int type;
+    V3 a, b, n, h;
+    Q4 rot;
+    float radius, friction;
+};
+
+__device__ __forceinline__ float signedDistance(const PrimF& P, V3 p, V3& n) {
+    if (P.type == 0) {
+        n = P.n;
+        return dot(p - P.a, P.n);
+    }
+    if (P.type == 1) return distanceToSphereLike(P.a, P.radius, p, n);
+    if (P.type == 2) {
+        const V3 ab = P.b - P.a;
+        const float len2 = norm2(ab);
+        const float t = len2 < 1e-30f ? 0.0f : clamp01(dot(p - P.a, ab) / len2);
+        const V3 axisPoint = P.a + (P.b - P.a) * t;
+        return distanceToSphereLike(axisPoint, P.radius, p, n);
+    }
+    // box
+    const V3 local = rotateInv(P.rot, p - P.a);
+    const V3 h = P.h;
+    const V3 clamped{clampT(local.x, -h.x, h.x), clampT(local.y, -h.y, h.y),
+                     clampT(local.z, -h.z, h.z)};
+    const V3 delta = local - clamped;
+    const float outside = norm(delta);
+    if (outside > 1e-12f) {
+        n = rotate(P.rot, divs(delta, outside));
+        return outside;
+    }
+    const float dx = h.x - absT(local.x);
+    const float dy = h.y - absT(local.y);
+    const float dz = h.z - absT(local.z);
+    V3 nn;
+    float depth;
+    if (dx <= dy && dx <= dz) {
+        nn = V3{local.x >= 0.0f ? 1.0f : -1.0f, 0.0f, 0.0f};
+        depth = dx;
+    } else if (dy <= dz) {
+        nn = V3{0.0f, local.y >= 0.0f ? 1.0f : -1.0f, 0.0f};
+        depth = dy;
+    } else {
+        nn = V3{0.0f, 0.0f, local.z >= 0.0f ? 1.0f : -1.0f};
+        depth = dz;
+    }
+    n = rotate(P.rot, nn);
+    return -depth;
+}
+
+// Closest points between segments [p1,q1] and [p2,q2] as parameters s, t.
+__device__ __forceinline__ void closestPointsBetweenSegments(V3 p1, V3 q1, V3 p2, V3 q2, float& s,
+                                                             float& t) {
+    const V3 d1 = q1 - p1, d2 = q2 - p2, r = p1 - p2;
+    const float a = norm2(d1), e = norm2(d2), f = dot(d2, r);
+    const float eps = 1e-30f;
+    if (a <= eps && e <= eps) {
+        s = t = 0.0f;
+        return;
+    }
+    if (a <= eps) {
+        s = 0.0f;
+        t = clamp01(f / e);
+        return;
+    }
+    const float c = dot(d1, r);
+    if (e <= eps) {
+        t = 0.0f;
+        s = clamp01(-c / a);
+        return;
+    }
+    const float b = dot(d1, d2);
+    const float denom = a * e - b * b;
+    s = denom > eps ? clamp01((b * f - c * e) / denom) : 0.0f;
+    t = (b * s + f) / e;
+    if (t < 0.0f) {
+        t = 0.0f;
+        s = clamp01(-c / a);
+    } else if (t > 1.0f) {
+        t = 1.0f;
+        s = clamp01((b - c) / a);
+    }
+}
+
+// Teschner et al. spatial hash of an integer cell (the reference's hashCell).
+__device__ __forceinline__ unsigned hashCell(int ix, int iy, int iz, int tableSize) {
+    const unsigned h = (static_cast<unsigned>(ix) * 73856093u) ^
+                       (static_cast<unsigned>(iy) * 19349663u) ^
+                       (static_cast<unsigned>(iz) * 83492791u);
+    return h % static_cast<unsigned>(tableSize);
+}
+__device__ __forceinline__ int cellCoord(float v, float cellSize) {
+    return static_cast<int>(floorf(v / cellSize));
+}
+
+__device__ __forceinline__ PrimF loadPrim(const DPrim& d) {
+    PrimF P;
+    P.type = static_cast<int>(d.typef);
+    P.a = V3{d.ax, d.ay, d.az};
+    P.b = V3{d.bx, d.by, d.bz};
+    P.n = V3{d.nx, d.ny, d.nz};
+    P.h = V3{d.hx, d.hy, d.hz};
+    P.rot = Q4{d.qw, d.qx, d.qy, d.qz};
+    P.radius = d.radius;
+    P.friction = d.friction;
+    return P;
+}
+
+}  // namespace rp

@@ -1,0 +1,405 @@
+// rp_step_common.cuh -- per-element operations of the XPBD Cosserat substep.
+//
+// Each function is one element of the reference algorithm, written against a
+// RodView whose arrays live wherever the calling kernel keeps them (shared
+// memory for the fused and batched forms, global memory for the multi-kernel
+// form). Because every strategy calls the same functions in the same order,
+// their results are bit-identical.
+//
+// Reference correspondence (FP32 GPU path / FP64 CPU path):
+//   projectStretchOne   gpu_solver.cu:49-76     solver.cpp:35-71
+//   projectBendOne      gpu_solver.cu:78-112    solver.cpp:81-123
+//   generateSlots       gpu_solver.cu:123-142   collision.cpp:90-101
+//   projectSlots        gpu_solver.cu:144-174   solver.cpp:163-216 (count 1)
+//   querySelfSegment    gpu_solver.cu:262-309   collision.cpp:119-151
+//   projectSelf         gpu_solver.cu:330-361   solver.cpp:163-216 (count 4)
+//   predict*/finish*    gpu_solver.cu:368-409   solver.cpp:223-266
+#pragma once
+
+#include "rp_internal.h"
+#include "rp_math.cuh"
+
+namespace rp {
+
+struct RodView {
+    // dynamic state (shared or global memory)
+    float4* x;
+    float4* xPrev;
+    float4* v;
+    float4* q;
+    float4* qPrev;
+    float4* omega;
+    float4* lamS;
+    float4* lamB;
+    float4* force;
+    float4* kin;
+    float4* torque;
+    float4* xComp;  // Kahan compensation (compensated precision only)
+    DSlot* slots;
+    // static template data (global memory, read-only)
+    const float* invMass;
+    const float4* invInertia;
+    const float4* inertia;
+    const int32_t* sP0;
+    const int32_t* sP1;
+    const int32_t* sSeg;
+    const float4* sComp;
+    const int32_t* bA;
+    const int32_t* bB;
+    const float4* bComp;
+    const float4* bRestD;
+    const DPrim* prims;
+    int numPrims;
+    float complianceScale;
+    float frictionScale;
+    float radius;
+    float contactMargin;
+};
+
+// Position update x[i] += d. In reference order this is a plain FP32 add. In
+// compensated mode (RP_PRECISION_COMPENSATED) x is a Kahan sum whose running
+// error lives in xComp (true position = x - xComp), and the xPrev array holds
+// the substep's displacement accumulator instead of the start position: a
+// small number carried at full relative precision, which is what friction and
+// velocity recovery need (position differences near 1 m lose everything below
+// ~6e-8 m in FP32).
+template <bool COMP>
+__device__ __forceinline__ void addPos(const RodView& V, int i, V3 d) {
+    if (!COMP) {
+        V.x[i] = f4(v3(V.x[i]) + d);
+    } else {
+        const float4 xs = V.x[i];
+        const float4 cs = V.xComp[i];
+        const V3 y = d - v3(cs);
+        const V3 t = v3(xs) + y;
+        const V3 c = (t - v3(xs)) - y;
+        V.x[i] = f4(t);
+        V.xComp[i] = f4(c);
+        V.xPrev[i] = f4(v3(V.xPrev[i]) + d);
+    }
+}
+
+// Displacement of particle i since the start of the substep.
+template <bool COMP>
+__device__ __forceinline__ V3 dispOf(const RodView& V, int i) {
+    return COMP ? v3(V.xPrev[i]) : v3(V.x[i]) - v3(V.xPrev[i]);
+}
+
+// ---------------------------------------------------------------- constraints
+
+template <bool COMP>
+__device__ __forceinline__ void projectStretchOne(const RodView& V, int k, float invH2) {
+    const int i0 = V.sP0[k], i1 = V.sP1[k], j = V.sSeg[k];
+    const float w0 = V.invMass[i0], w1 = V.invMass[i1];
+    const V3 iI = v3(V.invInertia[j]);
+    if (w0 == 0.0f && w1 == 0.0f && norm2(iI) == 0.0f) return;
+
+    const float4 sc = V.sComp[k];
+    const float l = sc.w;
+    const Q4 q = q4(V.q[j]);
+    V3 d = v3(V.x[i1]) - v3(V.x[i0]);
+    // compensated mode: the segment vector of the true (x - xComp) positions
+    if (COMP) d = d - (v3(V.xComp[i1]) - v3(V.xComp[i0]));
+    const V3 u = divs(rotateInv(q, d), l);
+    const V3 C = u - V3{0.0f, 0.0f, 1.0f};
+
+    const V3 alpha = v3(sc) * (invH2 * V.complianceScale);
+    M3 A = madd(midentity((w0 + w1) / (l * l)), sandwichDiag(mskew(u), iI));
+    A.m[0][0] += alpha.x;
+    A.m[1][1] += alpha.y;
+    A.m[2][2] += alpha.z;
+
+    const V3 lam = v3(V.lamS[k]);
+    V3 dL;
+    if (!solveSPD3(A, -(C + cwise(alpha, lam)), dL)) return;
+    V.lamS[k] = f4(lam + dL);
+
+    const V3 world = rotate(q, dL);
+    addPos<COMP>(V, i0, -(world * (w0 / l)));
+    addPos<COMP>(V, i1, world * (w1 / l));
+    if (norm2(iI) > 0.0f) V.q[j] = f4(applyBodyDelta(q, cwise(iI, cross(dL, u))));
+}
+
+__device__ __forceinline__ void projectBendOne(const RodView& V, int k, float invH2) {
+    const int a = V.bA[k], b = V.bB[k];
+    const V3 iIa = v3(V.invInertia[a]), iIb = v3(V.invInertia[b]);
+    if (norm2(iIa) == 0.0f && norm2(iIb) == 0.0f) return;
+
+    const float4 bc = V.bComp[k];
+    const float lbar = bc.w;
+    const Q4 qa = q4(V.q[a]);
+    const Q4 qb = q4(V.q[b]);
+    const Q4 p = sameHemisphereId(qmul(conj(qa), qb));
+    const V3 C = im(p) * (2.0f / lbar) - v3(V.bRestD[k]);
+
+    const M3 skewPv = mskew(im(p));
+    const M3 Ja = mscale(madd(midentity(-p.w), skewPv), 1.0f / lbar);
+    const M3 Jb = mscale(madd(midentity(p.w), skewPv), 1.0f / lbar);
+
+    const V3 alpha = v3(bc) * (invH2 * V.complianceScale);
+    M3 A = madd(sandwichDiag(Ja, iIa), sandwichDiag(Jb, iIb));
+    A.m[0][0] += alpha.x;
+    A.m[1][1] += alpha.y;
+    A.m[2][2] += alpha.z;
+
+    const V3 lam = v3(V.lamB[k]);
+    V3 dL;
+    if (!solveSPD3(A, -(C + cwise(alpha, lam)), dL)) return;
+    V.lamB[k] = f4(lam + dL);
+
+    if (norm2(iIa) > 0.0f) {
+        const V3 g = (dL * -p.w - cross(im(p), dL)) * (1.0f / lbar);
+        V.q[a] = f4(applyBodyDelta(qa, cwise(iIa, g)));
+    }
+    if (norm2(iIb) > 0.0f) {
+        const V3 g = (dL * p.w - cross(im(p), dL)) * (1.0f / lbar);
+        V.q[b] = f4(applyBodyDelta(qb, cwise(iIb, g)));
+    }
+}
+
+// ---------------------------------------------------------------- world contacts
+
+// Rebuild particle i's slots from its start-of-substep position, or between
+// regenerations only reset their multipliers.
+__device__ __forceinline__ void generateSlots(const RodView& V, int i, bool regenerate) {
+    const int base = i * V.numPrims;
+    const float w = V.invMass[i];
+    const V3 x = v3(V.x[i]);
+    for (int k = 0; k < V.numPrims; ++k) {
+        DSlot& c = V.slots[base + k];
+        c.lambdaN = 0.0f;
+        c.applied = 0.0f;
+        if (!regenerate) {
+            c.state = c.state != 0 ? 1 : 0;
+            continue;
+        }
+        c.state = 0;
+        if (w == 0.0f) continue;  // pinned: cannot respond
+        const PrimF P = loadPrim(V.prims[k]);
+        V3 n;
+        const float gap = signedDistance(P, x, n) - V.radius;
+        if (gap >= V.contactMargin) continue;
+        c.state = 1;
+        c.nx = n.x;
+        c.ny = n.y;
+        c.nz = n.z;
+        c.offset = dot(x, n) - gap;
+        c.friction = P.friction * V.frictionScale;
+    }
+}
+
+// Unilateral normal correction then position-level Coulomb friction, capped
+// on the total tangential correction of the substep. FP64 selects the
+// double-precision cone test (RP_PRECISION_FP64_CONE).
+template <bool COMP, bool FP64>
+__device__ __forceinline__ void projectSlots(const RodView& V, int i) {
+    const float w = V.invMass[i];
+    if (w <= 0.0f) return;
+    const int base = i * V.numPrims;
+    for (int k = 0; k < V.numPrims; ++k) {
+        DSlot& c = V.slots[base + k];
+        if (!c.state) continue;
+        const V3 n{c.nx, c.ny, c.nz};
+
+        const float C = dot(v3(V.x[i]), n) - c.offset;
+        float dLambda = -C / w;
+        const float clamped = c.lambdaN + dLambda > 0.0f ? c.lambdaN + dLambda : 0.0f;
+        dLambda = clamped - c.lambdaN;
+        c.lambdaN = clamped;
+        if (dLambda != 0.0f) addPos<COMP>(V, i, n * (w * dLambda));
+
+        if (c.friction <= 0.0f || c.lambdaN <= 0.0f) {
+            c.state = 1;
+            continue;
+        }
+        const V3 dp = dispOf<COMP>(V, i);
+        const V3 tangential = dp - n * dot(dp, n);
+        const float slide = norm(tangential);
+        if (slide < 1e-15f) {
+            c.state = 2;
+            continue;
+        }
+        if (!FP64) {
+            const float budget = c.friction * c.lambdaN * w - c.applied;
+            if (budget <= 0.0f) {
+                c.state = 3;
+                continue;
+            }
+            const float capped = slide < budget ? slide : budget;
+            c.state = slide <= budget ? 2 : 3;
+            c.applied += capped;
+            addPos<COMP>(V, i, tangential * (-capped / slide));
+        } else {
+            const double tx = tangential.x, ty = tangential.y, tz = tangential.z;
+            const double slideD = sqrt(tx * tx + ty * ty + tz * tz);
+            const double budget =
+                double(c.friction) * double(c.lambdaN) * double(w) - double(c.applied);
+            if (budget <= 0.0) {
+                c.state = 3;
+                continue;
+            }
+            const double capped = slideD < budget ? slideD : budget;
+            c.state = slideD <= budget ? 2 : 3;
+            c.applied = float(double(c.applied) + capped);
+            addPos<COMP>(V, i, tangential * float(-capped / slideD));
+        }
+    }
+}
+
+// ---------------------------------------------------------------- self contacts
+
+struct SelfScratch {
+    float4* centres;   // per segment
+    int32_t* cellOf;   // per segment
+    int32_t* sorted;   // per segment
+    int32_t* segCount; // per segment
+    int32_t* segStart; // per segment
+    int32_t* cellStart;// hashTableSize + 1
+    DSelf* pool;       // capacity
+    float* cellSize;   // 1
+    int32_t* live;     // 1
+    int32_t* overflow; // 1
+};
+
+// Contacts of segment j with later segments, in the reference's candidate
+// order (3x3x3 cells z/y/x, bucket order within a cell). fill = false counts
+// them into segCount[j]; fill = true writes them from segStart[j].
+__device__ __forceinline__ void querySelfSegment(const RodView& V, const SelfScratch& S, int j,
+                                                 int nSeg, int gap, int table, int capacity,
+                                                 float selfFriction, bool fill) {
+    int count = 0;
+    if (nSeg > gap) {
+        const float cell = *S.cellSize;
+        const V3 cj = v3(S.centres[j]);
+        const int cx = cellCoord(cj.x, cell), cy = cellCoord(cj.y, cell), cz = cellCoord(cj.z, cell);
+        const V3 a0 = v3(V.x[V.sP0[j]]), a1 = v3(V.x[V.sP1[j]]);
+        const float twoR = 2.0f * V.radius;
+        for (int dz = -1; dz <= 1; ++dz)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int h = int(hashCell(cx + dx, cy + dy, cz + dz, table));
+                    const int e1 = S.cellStart[h + 1];
+                    for (int e = S.cellStart[h]; e < e1; ++e) {
+                        const int k = S.sorted[e];
+                        if (k - j < gap) continue;
+                        const V3 b0 = v3(V.x[V.sP0[k]]), b1 = v3(V.x[V.sP1[k]]);
+                        float u, w;
+                        closestPointsBetweenSegments(a0, a1, b0, b1, u, w);
+                        const V3 delta = (a0 + (a1 - a0) * u) - (b0 + (b1 - b0) * w);
+                        const float dist = norm(delta);
+                        const float separation = dist - twoR;
+                        if (separation >= 0.0f) continue;
+                        const int slot = fill ? S.segStart[j] + count : 0;
+                        ++count;
+                        if (!fill || slot >= capacity) continue;
+                        DSelf& c = S.pool[slot];
+                        const V3 n = dist > 1e-12f ? divs(delta, dist) : V3{0.0f, 0.0f, 1.0f};
+                        c.nx = n.x;
+                        c.ny = n.y;
+                        c.nz = n.z;
+                        c.idx[0] = V.sP0[j];
+                        c.idx[1] = V.sP1[j];
+                        c.idx[2] = V.sP0[k];
+                        c.idx[3] = V.sP1[k];
+                        c.weight[0] = 1.0f - u;
+                        c.weight[1] = u;
+                        c.weight[2] = -(1.0f - w);
+                        c.weight[3] = -w;
+                        float dotSum = 0.0f;
+                        for (int m = 0; m < 4; ++m) dotSum += c.weight[m] * dot(v3(V.x[c.idx[m]]), n);
+                        c.offset = dotSum - separation;
+                        c.friction = selfFriction * V.frictionScale;
+                        c.lambdaN = 0.0f;
+                        c.applied = 0.0f;
+                        c.seg = (j << 16) | k;
+                    }
+                }
+    }
+    if (!fill) S.segCount[j] = count;
+}
+
+// The four-particle case of the contact projection.
+template <bool COMP>
+__device__ __forceinline__ void projectSelf(const RodView& V, DSelf& c) {
+    float wEff = 0.0f;
+    for (int m = 0; m < 4; ++m) wEff += c.weight[m] * c.weight[m] * V.invMass[c.idx[m]];
+    if (wEff <= 0.0f) return;
+    const V3 n{c.nx, c.ny, c.nz};
+
+    float C = -c.offset;
+    for (int m = 0; m < 4; ++m) C += c.weight[m] * dot(v3(V.x[c.idx[m]]), n);
+    float dLambda = -C / wEff;
+    const float clamped = c.lambdaN + dLambda > 0.0f ? c.lambdaN + dLambda : 0.0f;
+    dLambda = clamped - c.lambdaN;
+    c.lambdaN = clamped;
+    if (dLambda != 0.0f)
+        for (int m = 0; m < 4; ++m)
+            addPos<COMP>(V, c.idx[m], n * (V.invMass[c.idx[m]] * c.weight[m] * dLambda));
+
+    if (c.friction <= 0.0f || c.lambdaN <= 0.0f) return;
+
+    V3 dp{0.0f, 0.0f, 0.0f};
+    for (int m = 0; m < 4; ++m) {
+        const int pi = c.idx[m];
+        dp = dp + dispOf<COMP>(V, pi) * c.weight[m];
+    }
+    const V3 tangential = dp - n * dot(dp, n);
+    const float slide = norm(tangential);
+    if (slide < 1e-15f) return;
+    const float budget = c.friction * c.lambdaN * wEff - c.applied;
+    if (budget <= 0.0f) return;
+    const float capped = slide < budget ? slide : budget;
+    c.applied += capped;
+    const V3 correction = tangential * (-capped / slide);
+    for (int m = 0; m < 4; ++m)
+        addPos<COMP>(V, c.idx[m], correction * (V.invMass[c.idx[m]] * c.weight[m] / wEff));
+}
+
+// ---------------------------------------------------------------- predict / finish
+
+template <bool COMP>
+__device__ __forceinline__ void predictParticle(const RodView& V, int i, float h, V3 g) {
+    V.xPrev[i] = COMP ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : V.x[i];
+    const float w = V.invMass[i];
+    if (w == 0.0f) {
+        addPos<COMP>(V, i, v3(V.kin[i]) * h);  // prescribed motion
+        return;
+    }
+    const V3 vn = v3(V.v[i]) + (g + v3(V.force[i]) * w) * h;
+    V.v[i] = f4(vn);
+    addPos<COMP>(V, i, vn * h);
+}
+
+__device__ __forceinline__ void predictFrame(const RodView& V, int j, float h) {
+    const float4 qs = V.q[j];
+    V.qPrev[j] = qs;
+    const V3 iI = v3(V.invInertia[j]);
+    if (norm2(iI) == 0.0f) return;
+    const V3 w = v3(V.omega[j]);
+    const Q4 q = q4(qs);
+    const V3 tau = rotateInv(q, v3(V.torque[j]));
+    const V3 wn = w + cwise(iI, tau - cross(w, cwise(v3(V.inertia[j]), w))) * h;
+    V.omega[j] = f4(wn);
+    V.q[j] = f4(qnormalize(qadd(q, qscale(qmul(q, qmake(0.0f, wn)), 0.5f * h))));
+}
+
+template <bool COMP>
+__device__ __forceinline__ void finishParticle(const RodView& V, int i, float h, float linDecay) {
+    if (V.invMass[i] == 0.0f) {
+        V.v[i] = V.kin[i];
+        return;
+    }
+    const V3 d = dispOf<COMP>(V, i);
+    V.v[i] = f4(divs(d, h) * linDecay);
+}
+
+__device__ __forceinline__ void finishFrame(const RodView& V, int j, float h, float angDecay) {
+    if (norm2(v3(V.invInertia[j])) == 0.0f) {
+        V.omega[j] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        return;
+    }
+    const Q4 dq = sameHemisphereId(qmul(conj(q4(V.qPrev[j])), q4(V.q[j])));
+    V.omega[j] = f4(im(dq) * (2.0f / h) * angDecay);
+}
+
+}  // namespace rp

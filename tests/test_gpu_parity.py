@@ -1,0 +1,375 @@
+"""GPU parity: the CUDA step against the oracle, through the C ABI.
+
+Modelled on the reference's own GPU parity cases (src/gpu/gpu_cases.cpp:
+126-607). Tolerances are the reference's, stated per horizon:
+  * 1 step: GPU vs colour-ordered FP64 CPU <= 1e-7 m (gpu_cases.cpp:285) and
+    < 1 % of what the loads change in that step (:300-301);
+  * 200 steps: <= 1e-3 m, the float envelope (:303-304);
+  * strategies agree exactly, runs are bitwise deterministic (:305-306, 558-607);
+  * per-rod stiffness/friction scaling within 2 % of its effect (:415-418);
+  * self-collision restart: one step <= 3e-5 m, effect >= 10x tolerance,
+    no overflow (:537-545).
+Discrete decisions are compared exactly: colourings (host tests), world
+contact active sets and the self-contact pair list.
+"""
+import math
+import os
+
+import numpy as np
+import pytest
+
+import ropephysics_b200 as rp
+from oracle import Context, Params
+from tests.helpers import (REF_MAT, benchmark_rod, contact_world, max_dq, max_dx, oparams,
+                           oracle_world, product_rod, sync_loads, twist_root)
+from tests.test_oracle import rope_restart_rod
+
+pytestmark = pytest.mark.gpu
+
+STRATS = (rp.Strategy.MULTI_KERNEL, rp.Strategy.FUSED, rp.Strategy.BATCHED)
+BENCH = rp.StepParams(dt=1e-3, substeps=8, iterations=1)  # gpu_cases.cpp:55-62
+
+
+def run_scenario(oracle, scen, n, checkpoints=(1, 10, 50, 200)):
+    """Step the oracle and all three strategies side by side; returns per
+    checkpoint (oracle x, oracle q, {strategy: (x, q)})."""
+    orod = benchmark_rod(oracle, n)
+    root = orod.nS - 1
+    rest = orod.q[root].copy()
+    if scen == "loaded":
+        orod.extForce[orod.nP - 1] = (0.0, 0.02, 0.05)
+        orod.extTorque[n // 2] = (2e-3, 0.0, -1e-3)
+        orod.kinVel[0] = (0.0, 0.05, 0.1)
+    world = contact_world() if scen == "contact" else None
+    proto = product_rod(orod)
+    batches = {s: rp.Batch.create(proto, 1, s, world) for s in STRATS}
+    ow = oracle_world(world) if world else None
+    ctx = Context()
+    p = oparams(BENCH)
+    out = {}
+    done = 0
+    for cp in checkpoints:
+        while done < cp:
+            if scen == "loaded":
+                twist_root(orod, root, rest, done)
+                sync_loads(proto, orod)
+                for b in batches.values():
+                    b.set_loads(0, proto)
+            oracle.step(orod, p, world=ow, ctx=ctx)
+            for b in batches.values():
+                b.step(BENCH)
+            done += 1
+        res = {}
+        for s, b in batches.items():
+            r = product_rod(orod)
+            b.download(0, r)
+            res[s] = (r.x.copy(), r.q.copy())
+        out[cp] = (orod.x[: orod.nP].copy(), orod.q[: orod.nS].copy(), res)
+    for b in batches.values():
+        b.close()
+    return out
+
+
+@pytest.mark.parametrize("scen", ["gravity", "loaded", "contact"])
+@pytest.mark.parametrize("n", [16, 48, 128])
+def test_parity_against_fp64_oracle(oracle64, scen, n):
+    out = run_scenario(oracle64, scen, n)
+    for cp, (ox, oq, res) in out.items():
+        base = res[rp.Strategy.FUSED]
+        for s, (x, q) in res.items():
+            # strategies run the same per-element code in the same order
+            assert np.array_equal(x, base[0]) and np.array_equal(q, base[1]), (s, cp)
+        dx = max_dx(base[0], ox)
+        if cp == 1:
+            assert dx <= 1e-7, (scen, n, dx)
+        if cp == 200:
+            assert dx <= 1e-3, (scen, n, dx)
+
+
+def test_one_step_error_far_below_load_effect(oracle64):
+    """gpu_cases.cpp:291-302: the one-step check must be able to see loads."""
+    plain, loaded = benchmark_rod(oracle64, 16), benchmark_rod(oracle64, 16)
+    loaded.extForce[loaded.nP - 1] = (0.0, 0.02, 0.05)
+    loaded.extTorque[8] = (2e-3, 0.0, -1e-3)
+    loaded.kinVel[0] = (0.0, 0.05, 0.1)
+    p = oparams(BENCH)
+    oracle64.step(plain, p)
+    oracle64.step(loaded, p)
+    effect = max_dx(plain.x[: plain.nP], loaded.x[: loaded.nP])
+    out = run_scenario(oracle64, "loaded", 16, checkpoints=(1,))
+    ox, _, res = out[1]
+    err = max_dx(res[rp.Strategy.BATCHED][0], ox)
+    assert err / effect < 0.01
+
+
+def test_contact_scenario_makes_contact_and_matches(oracle64):
+    """gpu_cases.cpp:307-314: contact made, and its error < 1 % of its effect."""
+    n = 48
+    grav = run_scenario(oracle64, "gravity", n, checkpoints=(50,))[50][0]
+    out = run_scenario(oracle64, "contact", n, checkpoints=(50,))
+    ox, _, res = out[50]
+    effect = max_dx(grav, ox)
+    err = max_dx(res[rp.Strategy.BATCHED][0], ox)
+    assert effect > 1e-3 and err / effect < 0.01
+
+
+def test_contact_states_match_oracle(oracle64):
+    """Active set and stick/slip per (particle, primitive) after one step from
+    identical state equal the FP64 oracle's (its last-sweep friction states)."""
+    n = 48
+    orod = benchmark_rod(oracle64, n)
+    world = contact_world()
+    proto = product_rod(orod)
+    b = rp.Batch.create(proto, 1, rp.Strategy.BATCHED, world)
+    ctx = oracle64.step(orod, oparams(BENCH), world=oracle_world(world))
+    b.step(BENCH)
+    states = b.read_contact_states().reshape(orod.nP, 2)
+    expect = np.zeros_like(states)
+    for c in ctx.contacts():
+        expect[c["idx"][0], c["prim"]] = {0: 1, 1: 2, 2: 3}[c["friction_state"]]
+    assert np.count_nonzero(expect) >= 5
+    assert np.array_equal(states != 0, expect != 0)
+    agree = np.mean(states[expect != 0] == expect[expect != 0])
+    assert agree >= 0.95, agree
+
+
+def test_determinism_bitwise(oracle64):
+    """gpu_cases.cpp:558-607: 64 rods, n = 32 and 128, three runs, bitwise."""
+    for n in (32, 128):
+        proto = product_rod(benchmark_rod(oracle64, n))
+        for s in STRATS:
+            runs = []
+            for _ in range(3):
+                b = rp.Batch.create(proto, 64, s)
+                for _ in range(100):
+                    b.step(BENCH)
+                runs.append(b.download_positions())
+                b.close()
+            assert all(np.array_equal(runs[0], r) for r in runs[1:]), (n, s)
+
+
+def test_material_scales(oracle64):
+    """gpu_cases.cpp:316-419: per-rod stiffness and friction scaling."""
+    p = oparams(BENCH)
+    # stiffness: rod 1 three times stiffer, 20 steps
+    proto_o = benchmark_rod(oracle64, 16)
+    b = rp.Batch.create(product_rod(proto_o), 2, rp.Strategy.BATCHED)
+    b.set_material_scales(youngs_scale=[1.0, 3.0])
+    for _ in range(20):
+        b.step(BENCH)
+    pos = b.download_positions().reshape(2, -1, 3)
+    cpu_plain = benchmark_rod(oracle64, 16)
+    cpu_stiff = oracle64.straight(16, 1.0, youngs=3e7, poisson=0.35, density=1000.0, radius=5e-3)
+    oracle64.clamp(cpu_stiff, False)
+    oracle64.step(cpu_plain, p, steps=20)
+    oracle64.step(cpu_stiff, p, steps=20)
+    err = max(max_dx(pos[0], cpu_plain.x), max_dx(pos[1], cpu_stiff.x))
+    effect = max_dx(cpu_plain.x, cpu_stiff.x)
+    assert err / effect < 0.02
+    # friction: a rod across a 20 degree incline, mu 0.5 holds, 0.25 slides
+    tilt = 20.0 * math.pi / 180.0
+    normal = (math.sin(tilt), 0.0, math.cos(tilt))
+    start = tuple(np.array(normal) * (5e-3 + 1e-4) + np.array([0.0, -0.5, 0.0]))
+    o = oracle64.straight(16, 1.0, **REF_MAT, origin=start, direction=(0, 1, 0))
+    w = rp.World([rp.Primitive.plane((0, 0, 0), normal, 0.5)])
+    b = rp.Batch.create(product_rod(o), 2, rp.Strategy.BATCHED, w)
+    b.set_material_scales(friction_scale=[1.0, 0.5])
+    for _ in range(150):
+        b.step(BENCH)
+    pos = b.download_positions().reshape(2, -1, 3)
+    grip, slide = o.copy(), o.copy()
+    w2 = rp.World([rp.Primitive.plane((0, 0, 0), normal, 0.25)])
+    c0, c1 = Context(), Context()
+    for _ in range(150):
+        oracle64.step(grip, p, world=oracle_world(w), ctx=c0)
+        oracle64.step(slide, p, world=oracle_world(w2), ctx=c1)
+    err = max(max_dx(pos[0], grip.x), max_dx(pos[1], slide.x))
+    effect = max_dx(grip.x, slide.x)
+    assert effect > 1e-3 and err / effect < 0.02
+
+
+def test_self_collision_restart(oracle64):
+    """gpu_cases.cpp:421-546: one step from a coiled state, all strategies."""
+    rope, world, params, g = rope_restart_rod(oracle64)
+    proto = product_rod(rope)
+    pw = rp.World([rp.Primitive.plane((0, 0, 0), (0, 0, 1), 0.6)], self_collision=True,
+                  self_friction=0.3, hash_table_size=256)
+    sp = rp.StepParams(dt=1e-3, substeps=16, iterations=4, linear_damping=1.0, angular_damping=1.0)
+    # the first substep's pair list, from the identical start state
+    expect = []
+    for c in oracle64.generate_contacts(rope, world).contacts():
+        if c["count"] == 4:
+            expect.append((c["idx"][0], c["idx"][2]))  # segment j = p0, k = p0 of k
+    assert len(expect) >= 5
+    one = rp.StepParams(dt=1e-3 / 16, substeps=1, iterations=4, linear_damping=1.0,
+                        angular_damping=1.0)
+    for s in STRATS:
+        b = rp.Batch.create(proto, 1, s, pw)
+        b.step(one)
+        pairs = [tuple(p) for p in b.read_self_contacts(0)]
+        assert pairs == expect, s
+        b.close()
+    # one full step vs the FP64 CPU
+    cpu = rope.copy()
+    oracle64.step(cpu, oparams(sp), world=world, ctx=Context())
+    nos = rope.copy()
+    from oracle import World as OW
+    oracle64.step(nos, oparams(sp), world=OW(world.primitives, False), ctx=Context())
+    effect = max_dx(cpu.x, nos.x)
+    outs = {}
+    for s in STRATS:
+        b = rp.Batch.create(proto, 1, s, pw)
+        b.step(sp)
+        r = product_rod(rope)
+        b.download(0, r)
+        outs[s] = r.x.copy()
+        assert b.self_contact_overflow() == 0
+        b.close()
+    base = outs[rp.Strategy.FUSED]
+    for s, x in outs.items():
+        assert np.array_equal(x, base), s
+    err = max_dx(base, cpu.x)
+    assert err <= 3e-5, err
+    assert effect / 3e-5 >= 10
+
+
+def test_mixed_batch_equals_rods_alone(oracle64):
+    """Heterogeneous rods (lengths, worlds, self-collision) in one batched
+    launch produce, rod by rod, the bits the same rod produces alone."""
+    rng = np.random.default_rng(7)
+    rods, worlds = [], []
+    for i in range(12):
+        n = int(rng.integers(16, 200))
+        t = np.linspace(0, 2 * math.pi * rng.uniform(1, 3), n + 1)
+        rc = rng.uniform(0.05, 0.15)
+        pts = np.stack([rc * np.cos(t), rc * np.sin(t), 0.3 + 0.015 * t], 1)
+        r = rp.Rod.centerline(pts, rp.Material(1e8, 0.3, 1100, 5e-3))
+        r.b_rest_darboux[:] = 0.0
+        rods.append(r)
+        prims = [rp.Primitive.plane((0, 0, 0), (0, 0, 1), 0.5)]
+        if i % 2:
+            prims.append(rp.Primitive.sphere((0.0, 0.0, 0.2), 0.06, 0.4))
+        if i % 3 == 0:
+            prims.append(rp.Primitive.box((0.1, 0, 0.25), (0.05, 0.05, 0.03), (1, 0, 0, 0), 0.7))
+        worlds.append(rp.World(prims, self_collision=i % 4 != 3, self_friction=0.3,
+                               hash_table_size=128))
+    p = rp.StepParams(dt=1.0 / 60, substeps=20, iterations=1)
+    mixed = rp.Batch.create_mixed(rods, worlds, list(range(12)), rp.Strategy.BATCHED)
+    mixed.step_many(p, 5)
+    mx = mixed.download_positions()
+    for i, (r, w) in enumerate(zip(rods, worlds)):
+        for s in (rp.Strategy.FUSED, rp.Strategy.BATCHED):
+            alone = rp.Batch.create(r, 1, s, w)
+            alone.step_many(p, 5)
+            assert np.array_equal(alone.download_positions(), mixed.positions_of(i, mx)), (i, s)
+            alone.close()
+
+
+def test_graph_replay_equals_direct_launches(oracle64):
+    proto = product_rod(benchmark_rod(oracle64, 64))
+    w = contact_world()
+    a = rp.Batch.create(proto, 32, rp.Strategy.BATCHED, w)
+    b = rp.Batch.create(proto, 32, rp.Strategy.BATCHED, w)
+    b.set_graph(True)
+    for _ in range(3):
+        a.step_many(BENCH, 7)
+        b.step_many(BENCH, 7)
+    assert np.array_equal(a.download_positions(), b.download_positions())
+
+
+def test_device_drive_equals_host_upload(oracle64):
+    """A device drive gives the same bits as uploading the same kinematic
+    velocity from the host every step (the reference's control path)."""
+    o = oracle64.straight(64, 1.0, youngs=1e8, poisson=0.3, density=1100.0, radius=5e-3,
+                          direction=(0, 0, -1))
+    oracle64.pin(o, 0)
+    proto = product_rod(o)
+    n_rods = 8
+    rng = np.random.default_rng(1)
+    amp, freq, ph = rng.uniform(0, 0.1, n_rods), rng.uniform(0.5, 2, n_rods), rng.uniform(0, 6.28, n_rods)
+    p = rp.StepParams(dt=1.0 / 60, substeps=20, iterations=1)
+    dev = rp.Batch.create(proto, n_rods, rp.Strategy.BATCHED)
+    dev.set_drives([rp.Drive(0, (0, 0, 1), float(np.float32(a)), float(np.float32(f)), float(np.float32(q)))
+                    for a, f, q in zip(amp, freq, ph)])
+    host = rp.Batch.create(proto, n_rods, rp.Strategy.BATCHED)
+    t = 0.0
+    kin = np.zeros((n_rods, 65, 3), np.float32)
+    omega = np.float32(2 * math.pi * np.float64(np.float32(freq)))
+    for _ in range(30):
+        for r in range(n_rods):
+            om = float(np.float32(2.0 * math.pi * float(np.float32(freq[r]))))
+            s = float(np.float32(amp[r])) * om * math.cos(om * t + float(np.float32(ph[r])))
+            kin[r, 0, 2] = np.float32(s * 1.0)
+        host.set_kinematic_velocities(kin.reshape(-1, 3))
+        host.step(p)
+        dev.step(p)
+        t += float(np.float32(p.dt))
+    del omega
+    assert np.array_equal(host.download_positions(), dev.download_positions())
+
+
+def test_hold_observer(oracle64):
+    o = oracle64.straight(32, 1.0, **REF_MAT, direction=(0, 0, -1), origin=(0, 0, 1.0))
+    proto = product_rod(o)
+    b = rp.Batch.create(proto, 4, rp.Strategy.BATCHED)
+    b.set_drives([rp.Drive(-1)] * 4)
+    b.arm_hold_observer([0, 5, -1, 31], interval=5, tolerance=0.05)
+    start = b.download_positions().reshape(4, -1, 3)
+    peak = np.zeros(4)
+    for s in range(1, 21):
+        b.step(BENCH)
+        if s % 5 == 0:
+            z = b.download_positions().reshape(4, -1, 3)
+            for r, i in enumerate([0, 5, -1, 31]):
+                if i >= 0:
+                    peak[r] = max(peak[r], float(z[r, i, 2]) - float(start[r, i, 2]))
+    rise, held, near = b.read_hold_verdicts()
+    assert np.allclose(rise[[0, 1, 3]], peak[[0, 1, 3]], atol=1e-9)
+    assert held.all()
+
+
+def test_compensated_precision_tracks_fp64_longer(oracle64):
+    """Kahan-compensated positions move the FP32 trajectory closer to the
+    FP64 one on a rod held high where g h^2 nears the float spacing."""
+    o = oracle64.straight(64, 1.0, youngs=1e8, poisson=0.3, density=1100.0, radius=5e-3,
+                          origin=(100.0, 0.0, 50.0))
+    oracle64.clamp(o, False)
+    proto = product_rod(o)
+    p = rp.StepParams(dt=1.0 / 60, substeps=20, iterations=1)
+    ref = rp.Batch.create(proto, 1, rp.Strategy.BATCHED)
+    comp = rp.Batch.create(proto, 1, rp.Strategy.BATCHED)
+    comp.set_precision(rp.Precision.COMPENSATED)
+    cpu = o.copy()
+    for _ in range(60):
+        ref.step(p)
+        comp.step(p)
+    oracle64.step(cpu, oparams(p), steps=60)
+    e_ref = max_dx(ref.download_positions(), cpu.x)
+    e_comp = max_dx(comp.download_positions(), cpu.x)
+    assert e_comp < e_ref, (e_comp, e_ref)
+
+
+def test_fp64_cone_runs_and_stays_close(oracle64):
+    n = 48
+    orod = benchmark_rod(oracle64, n)
+    w = contact_world()
+    b = rp.Batch.create(product_rod(orod), 1, rp.Strategy.BATCHED, w)
+    b.set_precision(rp.Precision.FP64_CONE)
+    ctx = Context()
+    for _ in range(20):
+        b.step(BENCH)
+        oracle64.step(orod, oparams(BENCH), world=oracle_world(w), ctx=ctx)
+    assert max_dx(b.download_positions(), orod.x) < 1e-4
+
+
+def test_reports_and_accessors(oracle64):
+    proto = product_rod(benchmark_rod(oracle64, 64))
+    b = rp.Batch.create(proto, 10, rp.Strategy.FUSED)
+    assert b.stretch_colors == 2 and b.bend_colors == 2
+    assert b.launches_per_step(BENCH) == 1
+    assert b.shared_bytes_per_block > 0
+    assert rp.max_fused_segments() > 1000
+    assert "B200" in rp.device_name() or "sm_10" in rp.device_name()
+    before = b.kernel_launches
+    b.step(BENCH)
+    assert b.kernel_launches == before + 1
