@@ -334,6 +334,10 @@ int32_t rp_batch_launches_per_step(const rp_batch* batch, const rp_step_params* 
 int64_t rp_batch_self_contact_overflow(rp_batch* batch);
 /* Kernel launches issued by this batch since creation (for accounting). */
 int64_t rp_batch_kernel_launches(const rp_batch* batch);
+/* Rods whose kernels reported an internal inconsistency (a self-contact
+ * entry indexing outside its rod, which is then dropped instead of used);
+ * 0 in a correct run. -1 on a failed read. */
+int64_t rp_batch_error_count(rp_batch* batch);
 
 #ifdef __cplusplus
 }

@@ -427,6 +427,8 @@ class Reference:
         L.ref_rod_hanging.argtypes = [C.c_double, C.c_int, C.c_double, C.c_double, C.c_double,
                                       C.c_double]
         L.ref_rod_free.argtypes = [vp]
+        L.ref_rod_from.restype = vp
+        L.ref_rod_from.argtypes = [C.POINTER(OrcRod64)]
         L.ref_rod_clamp.argtypes = [vp, C.c_int]
         L.ref_rod_set_rest_from_current.argtypes = [vp]
         L.ref_rod_sizes.argtypes = [vp, C.POINTER(C.c_int)]
@@ -462,6 +464,22 @@ class Reference:
             L.refgpu_download_positions.argtypes = [vp, C.POINTER(C.c_float)]
             L.refgpu_overflow.restype = C.c_longlong
             L.refgpu_overflow.argtypes = [vp]
+            L.refgpu_self_pairs.argtypes = [vp, C.c_int, C.POINTER(C.c_int), C.c_int]
+            L.refgpu_contact_active.argtypes = [vp, C.c_int, C.POINTER(C.c_int)]
+
+    def gpu_self_pairs(self, batch, rod=0, cap=4096):
+        """(j, k) pairs of the reference GPU's last self-contact regeneration
+        (multi-kernel batches only)."""
+        out = np.zeros((cap, 2), np.int32)
+        n = self.lib.refgpu_self_pairs(batch, rod, out.ctypes.data_as(C.POINTER(C.c_int)), cap)
+        assert n >= 0, "reference batch is not multi-kernel or has no self-collision"
+        return [tuple(int(v) for v in p) for p in out[:n]]
+
+    def gpu_contact_active(self, batch, rod, num_particles, num_prims):
+        out = np.zeros(num_particles * num_prims, np.int32)
+        n = self.lib.refgpu_contact_active(batch, rod, out.ctypes.data_as(C.POINTER(C.c_int)))
+        assert n >= 0
+        return out.reshape(num_particles, num_prims)
 
     # --- rods (handles to crs::Rod) ---
     def straight(self, n, length, youngs=1e7, poisson=0.35, density=1000.0, radius=5e-3,
@@ -475,6 +493,10 @@ class Reference:
         return self.lib.ref_rod_centerline(pts.ctypes.data_as(C.POINTER(C.c_double)), len(pts),
                                            youngs, poisson, density, radius,
                                            Oracle._d3(frame_seed), float(twist_per_length))
+
+    def from_rod(self, rod: Rod):
+        """A reference Rod handle holding exactly `rod`'s arrays."""
+        return self.lib.ref_rod_from(C.byref(rod.c))
 
     def free(self, h):
         self.lib.ref_rod_free(h)

@@ -26,7 +26,18 @@
 #include "core/solver.h"
 #include "rod_oracle.h"
 #ifdef REF_WITH_GPU
+// The reference's GPU batch keeps its state private (gpu_solver.h:132-144,
+// gpu_batch.cpp:121-130). To read the discrete decisions its kernels made --
+// the self-contact pool and the world-contact active flags, which its
+// multi-kernel strategy leaves in global memory -- this test-only binding
+// compiles gpu_batch.cpp into its own translation unit with the members
+// visible. The standard headers are included first so only the reference's
+// header sees the visibility change.
+#include <string>
+#define private public
 #include "gpu/gpu_solver.h"
+#undef private
+#include "gpu/gpu_batch.cpp"
 #endif
 
 using namespace crs;
@@ -99,6 +110,62 @@ void* ref_rod_hanging(double length, int segments, double barRadius, double barH
     task.barHeight = barHeight;
     auto* h = new RodHandle();
     h->rod = task.build(legRatio, youngs);
+    return h;
+}
+
+// A reference Rod holding exactly an orc_rod's arrays (topology, rest data,
+// material and state).
+void* ref_rod_from(const orc_rod* o) {
+    auto* h = new RodHandle();
+    Rod& r = h->rod;
+    RodState& s = r.state;
+    r.material = material(o->youngs, o->poisson, o->density, o->radius);
+    s.x.resize(o->nP);
+    s.xPrev.resize(o->nP);
+    s.v.resize(o->nP);
+    s.invMass.resize(o->nP);
+    s.mass.resize(o->nP);
+    s.extForce.resize(o->nP);
+    s.kinematicVelocity.resize(o->nP);
+    for (int i = 0; i < o->nP; ++i) {
+        s.x[i] = get3(o->x, i);
+        s.xPrev[i] = get3(o->xPrev, i);
+        s.v[i] = get3(o->v, i);
+        s.invMass[i] = o->invMass[i];
+        s.mass[i] = o->mass[i];
+        s.extForce[i] = get3(o->extForce, i);
+        s.kinematicVelocity[i] = get3(o->kinVel, i);
+    }
+    s.q.resize(o->nS);
+    s.qPrev.resize(o->nS);
+    s.omega.resize(o->nS);
+    s.invInertia.resize(o->nS);
+    s.inertia.resize(o->nS);
+    s.extTorque.resize(o->nS);
+    for (int j = 0; j < o->nS; ++j) {
+        s.q[j] = get4(o->q, j);
+        s.qPrev[j] = get4(o->qPrev, j);
+        s.omega[j] = get3(o->omega, j);
+        s.invInertia[j] = get3(o->invInertia, j);
+        s.inertia[j] = get3(o->inertia, j);
+        s.extTorque[j] = get3(o->extTorque, j);
+    }
+    for (int k = 0; k < o->nSt; ++k) {
+        r.stretch.p0.push_back(o->sP0[k]);
+        r.stretch.p1.push_back(o->sP1[k]);
+        r.stretch.seg.push_back(o->sSeg[k]);
+        r.stretch.restLength.push_back(o->sRest[k]);
+        r.stretch.compliance.push_back(get3(o->sComp, k));
+        r.stretch.lambda.push_back(Vec3());
+    }
+    for (int k = 0; k < o->nB; ++k) {
+        r.bend.segA.push_back(o->bA[k]);
+        r.bend.segB.push_back(o->bB[k]);
+        r.bend.restLength.push_back(o->bRest[k]);
+        r.bend.restDarboux.push_back(get3(o->bRestD, k));
+        r.bend.compliance.push_back(get3(o->bComp, k));
+        r.bend.lambda.push_back(Vec3());
+    }
     return h;
 }
 
@@ -375,6 +442,41 @@ void refgpu_download_positions(void* b, float* out) {
     }
 }
 long long refgpu_overflow(void* b) { return static_cast<gpu::Batch*>(b)->selfContactOverflow(); }
+
+// Self-contact pairs (segment j, segment k) of the last regeneration, from
+// the multi-kernel strategy's global pool (gpu_kernels.h:125-134).
+int refgpu_self_pairs(void* bp, int rod, int* pairs, int cap) {
+    auto* b = static_cast<gpu::Batch*>(bp);
+    if (b->strategy_ != gpu::Strategy::kMultiKernel || !b->impl_->rod.selfCollision) return -1;
+    const gpu::DevStateF& st = b->impl_->state;
+    const gpu::DevRodF& d = b->impl_->rod;
+    int live = 0;
+    gpu::copyToHost(&live, st.selfLive + rod, sizeof(int));
+    std::vector<gpu::DevSelfContactF> pool(std::max(live, 1));
+    gpu::copyToHost(pool.data(), st.selfPool + std::size_t(rod) * d.selfCapacity,
+                    std::size_t(live) * sizeof(gpu::DevSelfContactF));
+    for (int c = 0; c < live && c < cap; ++c) {
+        // idx = (p0[j], p1[j], p0[k], p1[k]); for a chain p0[j] == j
+        pairs[2 * c] = pool[c].idx[0];
+        pairs[2 * c + 1] = pool[c].idx[2];
+    }
+    return live;
+}
+
+// World-contact active flags per (particle, primitive) of one rod, from the
+// multi-kernel strategy's element-major slots (gpu_batch.cpp:64-66).
+int refgpu_contact_active(void* bp, int rod, int* active) {
+    auto* b = static_cast<gpu::Batch*>(bp);
+    if (b->strategy_ != gpu::Strategy::kMultiKernel) return -1;
+    const gpu::DevRodF& d = b->impl_->rod;
+    const int nP = d.numParticles, np = d.numPrims, R = d.numRods;
+    if (np == 0) return 0;
+    std::vector<gpu::DevContactF> all(std::size_t(nP) * R * np);
+    gpu::copyToHost(all.data(), b->impl_->state.contacts, all.size() * sizeof(gpu::DevContactF));
+    for (int i = 0; i < nP; ++i)
+        for (int k = 0; k < np; ++k) active[i * np + k] = all[(std::size_t(i) * R + rod) * np + k].active;
+    return nP * np;
+}
 int refgpu_available() { return gpu::cudaAvailable() ? 1 : 0; }
 #endif
 

@@ -569,5 +569,8 @@ class Batch:
     def kernel_launches(self) -> int:
         return lib().rp_batch_kernel_launches(self._h)
 
+    def error_count(self) -> int:
+        return lib().rp_batch_error_count(self._h)
+
     def num_segments(self, rod_index: int = 0) -> int:
         return lib().rp_batch_num_segments(self._h, rod_index)

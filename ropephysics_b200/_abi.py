@@ -117,6 +117,7 @@ SIGNATURES = {
     "rp_batch_launches_per_step": (i32, [vp, P(StepParams)]),
     "rp_batch_self_contact_overflow": (i64, [vp]),
     "rp_batch_kernel_launches": (i64, [vp]),
+    "rp_batch_error_count": (i64, [vp]),
 }
 
 _lib = None

@@ -80,7 +80,8 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
     if failed:
         raise RuntimeError("compilation failed:\n" + "\n".join(failed))
     if jobs or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
-        cmd = [NVCC, "-shared"] + ARCH + ["-o", LIB] + objs + ["-lpthread"]
+        cmd = [NVCC, "-shared"] + ARCH + ["-Xlinker", "-soname=librp_b200.so", "-o", LIB] + objs + \
+            ["-lpthread"]
         r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
         if r.returncode != 0:
             sys.stdout.write(r.stdout)

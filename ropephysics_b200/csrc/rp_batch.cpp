@@ -513,11 +513,17 @@ static rp_status createImpl(const rp_rod_desc* const* rods, int numRods, const r
             ALLOC(A.gPool, rp::DSelf, size_t(b->totalPool));
         }
         ALLOC(A.gMisc, int32_t, 4 * size_t(numRods));
+    } else if (strategy == RP_STRATEGY_BATCHED) {
+        // the lean shared-memory layout keeps these in global memory
+        ALLOC(A.gqPrev, float4, S);
+        ALLOC(A.gSlots, rp::DSlot, size_t(b->totalSlots));
+        if (b->anySelf) ALLOC(A.gPool, rp::DSelf, size_t(b->totalPool));
     }
     ALLOC(A.contactState, uint8_t, size_t(b->totalSlots));
     ALLOC(A.selfCount, int32_t, numRods);
     ALLOC(A.selfOverflow, int32_t, numRods);
     ALLOC(A.selfPairs, int32_t, size_t(b->totalPool));
+    ALLOC(A.errors, int32_t, numRods);
     ALLOC(A.rodTime, double, numRods);
 #undef ALLOC
     A.numRods = numRods;
@@ -690,7 +696,7 @@ rp_status launchStep(rp_batch* b, const rp_step_params* p) {
         plan.threads = b->batchedThreads;
         plan.smemBytes = b->batchedSmem;
         e = rp::launchBatchedStep(A, plan, b->precision, b->stream);
-        b->launches += 2;
+        b->launches += 1;
     } else {
         A.work = nullptr;
         e = rp::launchPlainStep(A, b->strategy == RP_STRATEGY_MULTI_KERNEL, b->precision,
@@ -820,7 +826,7 @@ rp_status rp_batch_step_many(rp_batch* b, const rp_step_params* p, int32_t steps
         b->graphPrecision = b->precision;
     }
     RP_CUDA(cudaGraphLaunch(b->graphExec, b->stream));
-    b->launches += (b->strategy == RP_STRATEGY_BATCHED ? 2 : 1) * int64_t(steps);
+    b->launches += int64_t(steps);
     return RP_OK;
 }
 
@@ -1246,7 +1252,7 @@ size_t rp_batch_shared_bytes_per_block(const rp_batch* b) {
 }
 int32_t rp_batch_launches_per_step(const rp_batch* b, const rp_step_params*) {
     if (!b) return 0;
-    return b->strategy == RP_STRATEGY_BATCHED ? 2 : 1;
+    return 1;  // every strategy is one kernel per step
 }
 int64_t rp_batch_self_contact_overflow(rp_batch* b) {
     if (!b || !b->anySelf) return 0;
@@ -1262,5 +1268,19 @@ int64_t rp_batch_self_contact_overflow(rp_batch* b) {
     return t;
 }
 int64_t rp_batch_kernel_launches(const rp_batch* b) { return b ? b->launches : 0; }
+
+int64_t rp_batch_error_count(rp_batch* b) {
+    if (!b) return -1;
+    std::vector<int32_t> e(b->numRods);
+    if (cudaMemcpyAsync(e.data(), b->a.errors, e.size() * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                        b->stream) != cudaSuccess ||
+        cudaStreamSynchronize(b->stream) != cudaSuccess) {
+        fail(RP_ERR_CUDA, "error-word read failed");
+        return -1;
+    }
+    int64_t n = 0;
+    for (int32_t v : e) n += v != 0;
+    return n;
+}
 
 }  // extern "C"

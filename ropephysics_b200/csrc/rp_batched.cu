@@ -107,7 +107,7 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
     const RodLayout L = rodLayout(nP, nS, nSt, nB, R.numPrims, R.selfCollision, R.hashTableSize,
                                   R.selfCapacity, 1, COMP ? 1 : 0);
     V.q = reinterpret_cast<float4*>(base + L.q);
-    V.qPrev = reinterpret_cast<float4*>(base + L.qPrev);
+    V.qPrev = A.gqPrev + R.sOff;
     V.x = reinterpret_cast<float4*>(base + L.x);
     V.xPrev = reinterpret_cast<float4*>(base + L.xPrev);
     V.xComp = COMP ? reinterpret_cast<float4*>(base + L.xComp) : A.xComp + R.pOff;
@@ -119,7 +119,7 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
     V.torque = A.torque + R.sOff;
     V.lamS = reinterpret_cast<float4*>(base + L.lamS);
     V.lamB = reinterpret_cast<float4*>(base + L.lamB);
-    V.slots = reinterpret_cast<DSlot*>(base + L.slots);
+    V.slots = A.gSlots + R.slotOff;
     SelfScratch S;
     S.centres = reinterpret_cast<float4*>(base + L.centres);
     S.cellOf = reinterpret_cast<int32_t*>(base + L.selfInt);
@@ -128,12 +128,22 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
     S.segStart = S.segCount + nSt;
     S.cellStart = reinterpret_cast<int32_t*>(base + L.hash);
     int32_t* cursor = S.cellStart + (R.hashTableSize + 1);
-    S.pool = reinterpret_cast<DSelf*>(base + L.pool);
+    S.pool = A.gPool + R.poolOff;
     int32_t* misc = reinterpret_cast<int32_t*>(base + L.misc);
     S.cellSize = reinterpret_cast<float*>(misc);
     S.live = misc + 1;
     S.overflow = misc + 2;
     int32_t* partial = misc + 4;  // one per warp of the team (up to 8)
+    int32_t* numLevels = misc + 3;
+    unsigned long long* primMask = reinterpret_cast<unsigned long long*>(misc + 12);
+    float* red = reinterpret_cast<float*>(misc + 16);  // 8 floats per warp
+    int32_t* lvlOrder = reinterpret_cast<int32_t*>(base + L.levels);
+    int32_t* lvlStart = lvlOrder + (R.selfCapacity + 1);
+    int32_t* lvlOf = lvlStart + (R.selfCapacity + 1);
+    if (lane == 0) {
+        *numLevels = 0;
+        *primMask = ~0ull;
+    }
 
     int driveP = -1;
     float4 driveV = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -173,31 +183,69 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
         for (int k = lane; k < nSt; k += team) V.lamS[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         for (int k = lane; k < nB; k += team) V.lamB[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         const bool regenerate = sub % interval == 0;
-        if (V.numPrims > 0)
-            for (int i = lane; i < nP; i += team) generateSlots(V, i, regenerate);
-        if (self) {
-            if (regenerate) {
-                if (sub == 0 && lane == 0) *S.overflow = 0;
-                // centres and the longest segment
-                float mx = 0.0f;
+        if (regenerate && (V.numPrims > 0 || self)) {
+            // One pass for both contact kinds: segment centres and half
+            // lengths, the longest segment (self-collision cell size), and the
+            // rod's bounding box (primitive culling).
+            float mx = 0.0f;
+            float lx = 3.0e38f, ly = 3.0e38f, lz = 3.0e38f;
+            float hx = -3.0e38f, hy = -3.0e38f, hz = -3.0e38f;
+            if (self) {
                 for (int j = lane; j < nSt; j += team) {
                     const V3 a = v3(V.x[V.sP0[j]]), b = v3(V.x[V.sP1[j]]);
-                    S.centres[j] = f4((a + b) * 0.5f);
-                    mx = fmaxf(mx, norm(b - a));
+                    const float len = norm(b - a);
+                    const V3 c = (a + b) * 0.5f;
+                    S.centres[j] = make_float4(c.x, c.y, c.z, 0.5f * len);
+                    mx = fmaxf(mx, len);
                 }
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-                if ((lane & 31) == 0) reinterpret_cast<float*>(partial)[lane >> 5] = mx;
                 for (int t = lane; t <= table; t += team) S.cellStart[t] = 0;
-                teamSync(team, teamIdx);
-                float maxSegLen = 0.0f;
-                for (int w = 0; w < (team >> 5); ++w)
-                    maxSegLen = fmaxf(maxSegLen, reinterpret_cast<float*>(partial)[w]);
-                const float cell = maxSegLen + 2.0f * V.radius;
-                teamSync(team, teamIdx);  // partial is reused by the scan
-                if (lane == 0) *S.cellSize = cell;
+            }
+            if (V.numPrims > 0) {
+                for (int i = lane; i < nP; i += team) {
+                    const float4 p = V.x[i];
+                    lx = fminf(lx, p.x); ly = fminf(ly, p.y); lz = fminf(lz, p.z);
+                    hx = fmaxf(hx, p.x); hy = fmaxf(hy, p.y); hz = fmaxf(hz, p.z);
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+                lx = fminf(lx, __shfl_xor_sync(0xffffffffu, lx, o));
+                ly = fminf(ly, __shfl_xor_sync(0xffffffffu, ly, o));
+                lz = fminf(lz, __shfl_xor_sync(0xffffffffu, lz, o));
+                hx = fmaxf(hx, __shfl_xor_sync(0xffffffffu, hx, o));
+                hy = fmaxf(hy, __shfl_xor_sync(0xffffffffu, hy, o));
+                hz = fmaxf(hz, __shfl_xor_sync(0xffffffffu, hz, o));
+            }
+            if ((lane & 31) == 0) {
+                float* row = red + 8 * (lane >> 5);
+                row[0] = mx; row[1] = lx; row[2] = ly; row[3] = lz;
+                row[4] = hx; row[5] = hy; row[6] = hz;
+            }
+            teamSync(team, teamIdx);
+            for (int w = 0; w < (team >> 5); ++w) {
+                const float* row = red + 8 * w;
+                mx = fmaxf(mx, row[0]);
+                lx = fminf(lx, row[1]); ly = fminf(ly, row[2]); lz = fminf(lz, row[3]);
+                hx = fmaxf(hx, row[4]); hy = fmaxf(hy, row[5]); hz = fmaxf(hz, row[6]);
+            }
+            if (V.numPrims > 0 && lane == 0)
+                *primMask = primitivesNearBox(V, V3{lx, ly, lz}, V3{hx, hy, hz});
+            if (self && lane == 0) {
+                if (sub == 0) *S.overflow = 0;
+                *S.cellSize = mx + 2.0f * V.radius;
+            }
+            teamSync(team, teamIdx);  // mask and cell size visible; rows reusable
+        }
+        if (V.numPrims > 0) {
+            const unsigned long long mask = *primMask;
+            for (int i = lane; i < nP; i += team) generateSlotsMasked(V, i, regenerate, mask);
+        }
+        if (self) {
+            if (regenerate) {
+                const float cell = *S.cellSize;
                 for (int j = lane; j < nSt; j += team) {
-                    const V3 c = v3(S.centres[j]);
+                    const float4 c = S.centres[j];
                     const int h0 = int(hashCell(cellCoord(c.x, cell), cellCoord(c.y, cell),
                                                 cellCoord(c.z, cell), table));
                     S.cellOf[j] = h0;
@@ -228,17 +276,40 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
                 }
                 teamSync(team, teamIdx);
                 for (int j = lane; j < nSt; j += team)
-                    querySelfSegment(V, S, j, nSt, R.selfGap, table, R.selfCapacity, R.selfFriction, false);
+                    querySelfSegment<true>(V, S, j, nSt, R.selfGap, table, R.selfCapacity,
+                                           R.selfFriction, false);
                 teamSync(team, teamIdx);
                 for (int j = lane; j < nSt; j += team) S.segStart[j] = S.segCount[j];
                 teamSync(team, teamIdx);
                 const int total = teamExclusiveScan(S.segStart, nSt, lane, team, teamIdx, partial);
+                const int live = total < R.selfCapacity ? total : R.selfCapacity;
                 if (lane == 0) {
-                    *S.live = total < R.selfCapacity ? total : R.selfCapacity;
+                    *S.live = live;
                     if (total > R.selfCapacity) *S.overflow += total - R.selfCapacity;
                 }
-                for (int j = lane; j < nSt; j += team)
-                    querySelfSegment(V, S, j, nSt, R.selfGap, table, R.selfCapacity, R.selfFriction, true);
+                if (live > 0) {
+                    for (int j = lane; j < nSt; j += team)
+                        querySelfSegment<true>(V, S, j, nSt, R.selfGap, table, R.selfCapacity,
+                                               R.selfFriction, true);
+                    // every thread is done reading the hash (sorted) before
+                    // cellOf and sorted (2 nSt >= nP ints) are reused below
+                    teamSync(team, teamIdx);
+                    for (int i = lane; i < nP; i += team) S.cellOf[i] = 0;
+                    teamSync(team, teamIdx);
+                    if (lane == 0) {
+                        int kept = live;
+                        *numLevels = buildProjectionLevels(S.pool, live, nP, S.cellOf, lvlOf, lvlOrder,
+                                                           lvlStart, &kept);
+                        if (kept != live) {
+                            // a pool entry indexed outside the rod: keep the valid
+                            // prefix and report it, never touch memory with it
+                            *S.live = kept;
+                            if (A.errors) atomicOr(A.errors + r, 1);
+                        }
+                    }
+                } else if (lane == 0) {
+                    *numLevels = 0;
+                }
             } else if (lane == 0) {
                 for (int c = 0; c < *S.live; ++c) {
                     S.pool[c].lambdaN = 0.0f;
@@ -263,13 +334,19 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
                 teamSync(team, teamIdx);
             }
             if (V.numPrims > 0) {
-                for (int i = lane; i < nP; i += team) projectSlots<COMP, FP64>(V, i);
+                for (int i = lane; i < nP; i += team) projectSlots<COMP, FP64>(V, i, *primMask);
                 teamSync(team, teamIdx);
             }
             if (self) {
-                if (lane == 0)
-                    for (int c = 0; c < *S.live; ++c) projectSelf<COMP>(V, S.pool[c]);
-                teamSync(team, teamIdx);
+                // level by level: contacts of one level share no particle, and
+                // every earlier contact a contact shares a particle with sits in
+                // a lower level -- the serial pool order's result, bit for bit
+                const int nl = *numLevels;
+                for (int l = 0; l < nl; ++l) {
+                    for (int c = lvlStart[l] + lane; c < lvlStart[l + 1]; c += team)
+                        projectSelf<COMP>(V, S.pool[lvlOrder[c]]);
+                    teamSync(team, teamIdx);
+                }
             }
         }
 
@@ -292,7 +369,7 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
     if (V.numPrims > 0 && A.contactState) {
         const int slots = nP * V.numPrims;
         for (int s = lane; s < slots; s += team)
-            A.contactState[R.slotOff + s] = static_cast<uint8_t>(V.slots[s].state);
+            A.contactState[R.slotOff + s] = ((*primMask >> (s % V.numPrims)) & 1ull) ? static_cast<uint8_t>(V.slots[s].state) : uint8_t(0);
     }
     if (self) {
         const int live = *S.live;

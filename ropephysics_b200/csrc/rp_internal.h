@@ -141,6 +141,7 @@ struct DArgs {
     int32_t* selfCount;     // per rod: live pool entries after the last regeneration
     int32_t* selfOverflow;  // per rod, cumulative
     int32_t* selfPairs;     // per pool entry: (j << 16) | k
+    int32_t* errors;        // per rod: error bits set by the kernels (0 = none)
     double* rodTime;        // per rod simulated time (drives)
     const DDrive* drives;   // per rod, may be null
     DHold* hold;            // per rod, may be null

@@ -2,18 +2,22 @@
 // host (to size and validate the launch) and on the device (to carve it).
 //
 // Per rod, in bytes (16-byte aligned sections). The full layout (plain
-// kernel) stages every state array, as the reference's fused kernel does; the
-// lean layout (batched kernel) keeps only what the colour sweeps share between
-// threads -- positions, frames, their start-of-substep copies, multipliers,
-// contacts -- and leaves velocities, angular velocities and loads in global
-// memory, where predict and finish touch them once per substep.
-//   frames     q, qPrev [, omega, torque]           16 x nS each
-//   particles  x, xPrev [, v, force, kin], xComp    16 x nP each (xComp: full,
-//                                                   or lean with compensation)
-//   lambdas    stretch, bend                        16 x (nSt + nB)
-//   slots      world contacts                       32 x nP x numPrims
-//   self       centres 16 nSt, ints 16 nSt, misc 64, hash + cursor
-//              2 x 4 (table + 1), pool 64 x capacity
+// kernel) stages every state array, as the reference's fused kernel does. The
+// lean layout (batched kernel) keeps only what the colour sweeps and the
+// self-collision broad phase read many times per substep -- positions and
+// their start-of-substep copies, frames, multipliers, the hash -- and leaves
+// in global memory what is touched once or twice per substep (velocities,
+// angular velocities, loads, qPrev) or only when a contact is live (world
+// contact slots of primitives that survive the per-rod cull, the self-contact
+// pool); those stay L1/L2-resident.
+//   frames     q [, qPrev, omega, torque]            16 x nS each
+//   particles  x, xPrev [, v, force, kin], xComp     16 x nP each (xComp: full,
+//                                                    or lean with compensation)
+//   lambdas    stretch, bend                         16 x (nSt + nB)
+//   slots      [world contacts]                      32 x nP x numPrims
+//   misc       kMiscBytes (below)
+//   self       centres 16 nSt, ints 16 nSt, hash + cursor 2 x 4 (table + 1),
+//              [pool 64 x capacity], projection levels 3 x 4 (capacity + 1)
 #pragma once
 
 #include <cstdint>
@@ -31,9 +35,15 @@ struct RodLayout {
     int32_t x, xPrev, v, force, kin, xComp;
     int32_t lamS, lamB;
     int32_t slots;
-    int32_t centres, selfInt, misc, hash, pool;
+    int32_t centres, selfInt, misc, hash, pool, levels;
     int32_t bytes;
 };
+
+// Per-rod scalars and team reduction scratch, as 32-bit words:
+//   [0] cell size  [1] live pool entries  [2] overflow  [3] projection levels
+//   [4..11] per-warp scan partials  [12..13] primitive mask (64 bits)
+//   [16..79] per-warp reduction rows (8 warps x 8 floats)
+constexpr int32_t kMiscBytes = 320;
 
 RP_HD inline int32_t rpAlign16(int32_t b) { return (b + 15) & ~15; }
 
@@ -43,7 +53,11 @@ RP_HD inline RodLayout rodLayout(int32_t nP, int32_t nS, int32_t nSt, int32_t nB
     RodLayout L;
     int32_t o = 0;
     L.q = o;      o += 16 * nS;
-    L.qPrev = o;  o += 16 * nS;
+    if (!lean) {
+        L.qPrev = o;  o += 16 * nS;
+    } else {
+        L.qPrev = -1;
+    }
     L.x = o;      o += 16 * nP;
     L.xPrev = o;  o += 16 * nP;
     if (!lean) {
@@ -62,15 +76,24 @@ RP_HD inline RodLayout rodLayout(int32_t nP, int32_t nS, int32_t nSt, int32_t nB
     }
     L.lamS = o;   o += 16 * nSt;
     L.lamB = o;   o += 16 * nB;
-    L.slots = o;  o += 32 * nP * nPrims;
+    if (!lean) {
+        L.slots = o;  o += 32 * nP * nPrims;
+    } else {
+        L.slots = -1;
+    }
+    L.misc = o;        o += kMiscBytes;
     if (self) {
         L.centres = o; o += 16 * nSt;
         L.selfInt = o; o += 16 * nSt;
-        L.misc = o;    o += 64;
         L.hash = o;    o += rpAlign16(8 * (table + 1));
-        L.pool = o;    o += 64 * capacity;
+        if (!lean) {
+            L.pool = o;    o += 64 * capacity;
+        } else {
+            L.pool = -1;
+        }
+        L.levels = o;  o += rpAlign16(12 * (capacity + 1));
     } else {
-        L.centres = L.selfInt = L.misc = L.hash = L.pool = o;
+        L.centres = L.selfInt = L.hash = L.pool = L.levels = o;
     }
     L.bytes = o;
     return L;

@@ -256,7 +256,9 @@ __device__ __forceinline__ unsigned hashCell(int ix, int iy, int iz, int tableSi
     const unsigned h = (static_cast<unsigned>(ix) * 73856093u) ^
                        (static_cast<unsigned>(iy) * 19349663u) ^
                        (static_cast<unsigned>(iz) * 83492791u);
-    return h % static_cast<unsigned>(tableSize);
+    // h % tableSize; for a power-of-two table the mask is the same number
+    const unsigned t = static_cast<unsigned>(tableSize);
+    return (t & (t - 1u)) == 0u ? (h & (t - 1u)) : h % t;
 }
 __device__ __forceinline__ int cellCoord(float v, float cellSize) {
     return static_cast<int>(floorf(v / cellSize));

@@ -200,7 +200,7 @@ __global__ void __launch_bounds__(128, 4) kPlainStep(DArgs A) {
                 }
                 __syncthreads();
                 for (int j = tid; j < nSt; j += nth)
-                    querySelfSegment(V, S, j, nSt, R.selfGap, R.hashTableSize, R.selfCapacity,
+                    querySelfSegment<false>(V, S, j, nSt, R.selfGap, R.hashTableSize, R.selfCapacity,
                                      R.selfFriction, false);
                 __syncthreads();
                 if (tid == 0) {
@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(128, 4) kPlainStep(DArgs A) {
                 }
                 __syncthreads();
                 for (int j = tid; j < nSt; j += nth)
-                    querySelfSegment(V, S, j, nSt, R.selfGap, R.hashTableSize, R.selfCapacity,
+                    querySelfSegment<false>(V, S, j, nSt, R.selfGap, R.hashTableSize, R.selfCapacity,
                                      R.selfFriction, true);
             } else if (tid == 0) {
                 for (int c = 0; c < *S.live; ++c) {
@@ -240,7 +240,7 @@ __global__ void __launch_bounds__(128, 4) kPlainStep(DArgs A) {
                 __syncthreads();
             }
             if (V.numPrims > 0) {
-                for (int i = tid; i < nP; i += nth) projectSlots<COMP, FP64>(V, i);
+                for (int i = tid; i < nP; i += nth) projectSlots<COMP, FP64>(V, i, ~0ull);
                 __syncthreads();
             }
             if (self) {

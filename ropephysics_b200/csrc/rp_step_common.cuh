@@ -188,15 +188,87 @@ __device__ __forceinline__ void generateSlots(const RodView& V, int i, bool rege
     }
 }
 
+// Bit k set when primitive k may lie within reach (rod radius + contact
+// margin) of some particle in the box [lo, hi]. A primitive is dropped only
+// when a bound on its distance -- the plane's distance to the box, or the
+// distance from the box to a sphere that contains the primitive -- exceeds
+// the reach by a slack far above FP32 error, so no particle it drops could
+// have produced a contact: generation with the mask equals generation
+// without it.
+__device__ __forceinline__ unsigned long long primitivesNearBox(const RodView& V, V3 lo, V3 hi) {
+    const V3 c = (lo + hi) * 0.5f;
+    const V3 e = (hi - lo) * 0.5f;
+    const float reach = V.radius + V.contactMargin;
+    const float slack = 1e-3f * fabsf(reach) + 1e-4f +
+                        1e-5f * (fabsf(c.x) + fabsf(c.y) + fabsf(c.z) + e.x + e.y + e.z);
+    unsigned long long mask = 0ull;
+    for (int k = 0; k < V.numPrims && k < 64; ++k) {
+        const PrimF P = loadPrim(V.prims[k]);
+        bool near;
+        if (P.type == 0) {
+            const float s = dot(c - P.a, P.n) -
+                            (fabsf(P.n.x) * e.x + fabsf(P.n.y) * e.y + fabsf(P.n.z) * e.z);
+            near = s <= reach + slack;
+        } else {
+            V3 centre = P.a;
+            float rho = P.radius;
+            if (P.type == 2) {
+                centre = (P.a + P.b) * 0.5f;
+                rho = 0.5f * norm(P.b - P.a) + P.radius;
+            } else if (P.type == 3) {
+                rho = norm(P.h);
+            }
+            const V3 d{fmaxf(fabsf(centre.x - c.x) - e.x, 0.0f), fmaxf(fabsf(centre.y - c.y) - e.y, 0.0f),
+                       fmaxf(fabsf(centre.z - c.z) - e.z, 0.0f)};
+            near = norm(d) - rho <= reach + slack;
+        }
+        if (near) mask |= 1ull << k;
+    }
+    return mask;
+}
+
+// generateSlots for the primitives in `mask`. The slots of the others are not
+// touched: they hold no contact, and every reader (projection, the state
+// output) consults the same mask.
+__device__ __forceinline__ void generateSlotsMasked(const RodView& V, int i, bool regenerate,
+                                                    unsigned long long mask) {
+    const int base = i * V.numPrims;
+    const float w = V.invMass[i];
+    const V3 x = v3(V.x[i]);
+    for (int k = 0; k < V.numPrims; ++k) {
+        if (!((mask >> k) & 1ull)) continue;
+        DSlot& c = V.slots[base + k];
+        c.lambdaN = 0.0f;
+        c.applied = 0.0f;
+        if (!regenerate) {
+            c.state = c.state != 0 ? 1 : 0;
+            continue;
+        }
+        c.state = 0;
+        if (w == 0.0f) continue;
+        const PrimF P = loadPrim(V.prims[k]);
+        V3 n;
+        const float gap = signedDistance(P, x, n) - V.radius;
+        if (gap >= V.contactMargin) continue;
+        c.state = 1;
+        c.nx = n.x;
+        c.ny = n.y;
+        c.nz = n.z;
+        c.offset = dot(x, n) - gap;
+        c.friction = P.friction * V.frictionScale;
+    }
+}
+
 // Unilateral normal correction then position-level Coulomb friction, capped
 // on the total tangential correction of the substep. FP64 selects the
 // double-precision cone test (RP_PRECISION_FP64_CONE).
 template <bool COMP, bool FP64>
-__device__ __forceinline__ void projectSlots(const RodView& V, int i) {
+__device__ __forceinline__ void projectSlots(const RodView& V, int i, unsigned long long mask) {
     const float w = V.invMass[i];
     if (w <= 0.0f) return;
     const int base = i * V.numPrims;
     for (int k = 0; k < V.numPrims; ++k) {
+        if (!((mask >> k) & 1ull)) continue;
         DSlot& c = V.slots[base + k];
         if (!c.state) continue;
         const V3 n{c.nx, c.ny, c.nz};
@@ -264,16 +336,26 @@ struct SelfScratch {
 // Contacts of segment j with later segments, in the reference's candidate
 // order (3x3x3 cells z/y/x, bucket order within a cell). fill = false counts
 // them into segCount[j]; fill = true writes them from segStart[j].
+//
+// PREFILTER (batched form) rejects a candidate before the closest-point solve
+// when the segments' bounding spheres (centre, half length in centres[].w)
+// are apart by more than 2r plus a slack of 1e-3 of the bound plus 1e-6 of
+// the coordinate magnitude -- orders of magnitude above the FP32 error of the
+// solve -- so every pair it rejects is one the solve would reject too, and
+// the pair list is unchanged.
+template <bool PREFILTER>
 __device__ __forceinline__ void querySelfSegment(const RodView& V, const SelfScratch& S, int j,
                                                  int nSeg, int gap, int table, int capacity,
                                                  float selfFriction, bool fill) {
     int count = 0;
     if (nSeg > gap) {
         const float cell = *S.cellSize;
-        const V3 cj = v3(S.centres[j]);
+        const float4 cj4 = S.centres[j];
+        const V3 cj = v3(cj4);
         const int cx = cellCoord(cj.x, cell), cy = cellCoord(cj.y, cell), cz = cellCoord(cj.z, cell);
         const V3 a0 = v3(V.x[V.sP0[j]]), a1 = v3(V.x[V.sP1[j]]);
         const float twoR = 2.0f * V.radius;
+        const float scaleSlack = 1e-6f * (1.0f + fabsf(cj.x) + fabsf(cj.y) + fabsf(cj.z));
         for (int dz = -1; dz <= 1; ++dz)
             for (int dy = -1; dy <= 1; ++dy)
                 for (int dx = -1; dx <= 1; ++dx) {
@@ -282,6 +364,13 @@ __device__ __forceinline__ void querySelfSegment(const RodView& V, const SelfScr
                     for (int e = S.cellStart[h]; e < e1; ++e) {
                         const int k = S.sorted[e];
                         if (k - j < gap) continue;
+                        if (PREFILTER) {
+                            const float4 ck = S.centres[k];
+                            const float ddx = ck.x - cj.x, ddy = ck.y - cj.y, ddz = ck.z - cj.z;
+                            const float bound = cj4.w + ck.w + twoR;
+                            const float lim = bound * 1.001f + scaleSlack;
+                            if (ddx * ddx + ddy * ddy + ddz * ddz > lim * lim) continue;
+                        }
                         const V3 b0 = v3(V.x[V.sP0[k]]), b1 = v3(V.x[V.sP1[k]]);
                         float u, w;
                         closestPointsBetweenSegments(a0, a1, b0, b1, u, w);
@@ -316,6 +405,48 @@ __device__ __forceinline__ void querySelfSegment(const RodView& V, const SelfScr
                 }
     }
     if (!fill) S.segCount[j] = count;
+}
+
+// Levels for projecting a self-contact pool in parallel with the serial
+// pool order's result: level(c) = 1 + the highest level among earlier
+// contacts that share a particle with c. Contacts of one level touch disjoint
+// particles, and every earlier contact that c depends on sits in a lower
+// level, so projecting level by level computes exactly what the serial loop
+// computes. `last` holds one zeroed int per particle; `lvlOf` one int per
+// contact. Fills order[live] (contacts grouped by level, pool order within a
+// level) and start[levels + 1]; returns the number of levels. Entries whose
+// particle indices fall outside [0, nP) are never dereferenced: the pool is
+// cut before the first of them and *kept says how many entries remain. One
+// thread.
+__device__ __forceinline__ int buildProjectionLevels(const DSelf* pool, int live, int nP, int32_t* last,
+                                                     int32_t* lvlOf, int32_t* order, int32_t* start,
+                                                     int* kept) {
+    for (int c = 0; c < live; ++c) {
+        const DSelf& k = pool[c];
+        bool ok = true;
+        for (int m = 0; m < 4; ++m) ok = ok && k.idx[m] >= 0 && k.idx[m] < nP;
+        if (!ok) {
+            live = c;
+            break;
+        }
+    }
+    *kept = live;
+    int levels = 0;
+    for (int c = 0; c < live; ++c) {
+        const DSelf& k = pool[c];
+        int l = 0;
+        for (int m = 0; m < 4; ++m) l = max(l, last[k.idx[m]]);
+        lvlOf[c] = l;
+        for (int m = 0; m < 4; ++m) last[k.idx[m]] = l + 1;
+        levels = max(levels, l + 1);
+    }
+    for (int l = 0; l <= levels; ++l) start[l] = 0;
+    for (int c = 0; c < live; ++c) ++start[lvlOf[c] + 1];
+    for (int l = 0; l < levels; ++l) start[l + 1] += start[l];
+    for (int c = 0; c < live; ++c) order[start[lvlOf[c]]++] = c;
+    for (int l = levels; l > 0; --l) start[l] = start[l - 1];
+    start[0] = 0;
+    return levels;
 }
 
 // The four-particle case of the contact projection.

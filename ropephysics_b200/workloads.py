@@ -106,24 +106,47 @@ def _random_quat(rng):
     return tuple(q / np.linalg.norm(q))
 
 
-def _random_primitive(rng, centre, mu):
-    kind = int(rng.integers(1, 4))  # sphere, capsule, box
-    d = rng.normal(size=3)
-    d = d / np.linalg.norm(d) * rng.uniform(0.0, 1.0) ** (1.0 / 3.0)
-    c = tuple(np.asarray(centre) + d)
-    if kind == 1:
-        return Primitive.sphere(c, float(rng.uniform(0.02, 0.2)), mu)
-    if kind == 2:
-        axis = rng.normal(size=3)
-        axis = axis / np.linalg.norm(axis) * rng.uniform(0.1, 0.5) * 0.5
-        return Primitive.capsule(tuple(np.asarray(c) - axis), tuple(np.asarray(c) + axis),
-                                 float(rng.uniform(0.01, 0.05)), mu)
-    return Primitive.box(c, tuple(rng.uniform(0.05, 0.3, 3)), _random_quat(rng), mu)
+def _random_primitive(rng, centre, mu, lo, hi, clearance=0.02, tries=64):
+    """A sphere, capsule or box centred within 1 m of `centre` whose bounding
+    sphere keeps `clearance` from the rod's box [lo, hi] (no rod starts inside
+    a primitive)."""
+    for _ in range(tries):
+        kind = int(rng.integers(1, 4))  # sphere, capsule, box
+        d = rng.normal(size=3)
+        d = d / np.linalg.norm(d) * rng.uniform(0.0, 1.0) ** (1.0 / 3.0)
+        c = np.asarray(centre) + d
+        if kind == 1:
+            r = float(rng.uniform(0.02, 0.2))
+            prim, bound = Primitive.sphere(tuple(c), r, mu), r
+        elif kind == 2:
+            axis = rng.normal(size=3)
+            half = rng.uniform(0.1, 0.5) * 0.5
+            axis = axis / np.linalg.norm(axis) * half
+            r = float(rng.uniform(0.01, 0.05))
+            prim = Primitive.capsule(tuple(c - axis), tuple(c + axis), r, mu)
+            bound = half + r
+        else:
+            h = rng.uniform(0.05, 0.3, 3)
+            prim, bound = Primitive.box(tuple(c), tuple(h), _random_quat(rng), mu), float(np.linalg.norm(h))
+        gap = np.linalg.norm(np.maximum(np.abs(c - (lo + hi) / 2) - (hi - lo) / 2, 0.0)) - bound
+        if gap >= clearance:
+            return prim
+    return prim
+
+
+def table_for(segments: int, lo: int = 64, hi: int = 1024) -> int:
+    """Spatial-hash table size for a rod: the power of two >= 2 x segments,
+    clamped to [lo, hi] (few bucket collisions, bounded shared memory)."""
+    t = lo
+    while t < 2 * segments and t < hi:
+        t *= 2
+    return t
 
 
 def uneven(num_rods: int = 16384, seed: int = 0, min_seg: int = 16, max_seg: int = 512,
-           substeps: int = 50, hash_table_size: int = 256) -> Workload:
-    """Uneven batch: rods of 16..512 segments, coiled, each with its own world."""
+           substeps: int = 50, hash_table_size: int = 0) -> Workload:
+    """Uneven batch: rods of 16..512 segments, coiled, each with its own world.
+    hash_table_size 0 sizes each rod's table with table_for()."""
     rng = np.random.default_rng(seed)
     rods, worlds = [], []
     for _ in range(num_rods):
@@ -137,11 +160,13 @@ def uneven(num_rods: int = 16384, seed: int = 0, min_seg: int = 16, max_seg: int
         rods.append(rod)
         mu = float(rng.uniform(0.2, 1.0))
         centre = pts.mean(axis=0)
-        prims = [_random_primitive(rng, centre, mu) for _ in range(int(rng.integers(1, 5)))]
-        worlds.append(World(prims, self_collision=True, self_friction=mu, hash_table_size=hash_table_size))
+        lo, hi = pts.min(axis=0), pts.max(axis=0)
+        prims = [_random_primitive(rng, centre, mu, lo, hi) for _ in range(int(rng.integers(1, 5)))]
+        worlds.append(World(prims, self_collision=True, self_friction=mu,
+                            hash_table_size=hash_table_size or table_for(n)))
     return Workload(f"uneven-{num_rods}x[{min_seg},{max_seg}]", rods, worlds, list(range(num_rods)),
                     StepParams(dt=1.0 / 60, substeps=substeps, iterations=1), steps=500,
-                    info=dict(seed=seed, hash_table_size=hash_table_size))
+                    info=dict(seed=seed, hash_table_size=hash_table_size or "2n, pow2, 64..1024"))
 
 
 def hanging_cable_points(leg_ratio: float, length=1.2, segments=120, bar_radius=0.02,

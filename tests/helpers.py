@@ -102,6 +102,23 @@ def twisted_root(step_index, rest_q):
     return np.array([c * s for c in q])
 
 
+def segment_distance(p1, q1, p2, q2) -> float:
+    """Distance between the closest points of two segments (FP64, clamped
+    parametric solution of geometry.h:170-207)."""
+    p1, q1, p2, q2 = (np.asarray(v, np.float64) for v in (p1, q1, p2, q2))
+    d1, d2, r = q1 - p1, q2 - p2, p1 - p2
+    a, e, f = d1 @ d1, d2 @ d2, d2 @ r
+    c, b = d1 @ r, d1 @ d2
+    denom = a * e - b * b
+    s = min(max((b * f - c * e) / denom, 0.0), 1.0) if denom > 1e-30 else 0.0
+    t = (b * s + f) / e
+    if t < 0.0:
+        t, s = 0.0, min(max(-c / a, 0.0), 1.0)
+    elif t > 1.0:
+        t, s = 1.0, min(max((b - c) / a, 0.0), 1.0)
+    return float(np.linalg.norm((p1 + d1 * s) - (p2 + d2 * t)))
+
+
 def helix_points(n, length, coil_radius, pitch_gap, radius, origin=(0.0, 0.0, 0.0)):
     """n+1 points on a helix of total arc length `length` whose turns are
     separated by `pitch_gap` + 2 radius along the axis."""

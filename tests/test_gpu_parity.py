@@ -195,20 +195,30 @@ def test_self_collision_restart(oracle64):
     pw = rp.World([rp.Primitive.plane((0, 0, 0), (0, 0, 1), 0.6)], self_collision=True,
                   self_friction=0.3, hash_table_size=256)
     sp = rp.StepParams(dt=1e-3, substeps=16, iterations=4, linear_damping=1.0, angular_damping=1.0)
-    # the first substep's pair list, from the identical start state
-    expect = []
-    for c in oracle64.generate_contacts(rope, world).contacts():
-        if c["count"] == 4:
-            expect.append((c["idx"][0], c["idx"][2]))  # segment j = p0, k = p0 of k
-    assert len(expect) >= 5
+    # The first substep's pair list from the identical start state. Float and
+    # double legitimately disagree on pairs at the contact threshold (the
+    # reference measured 6 vs 8 self contacts at this restart,
+    # gpu_cases.cpp:429-436): against FP64 every disagreement must be a pair
+    # within 1e-6 m of touching. The exact comparison (same pairs, same order)
+    # is in test_gpu_reference.py, against the reference's own FP32 kernel.
+    f64 = [(c["idx"][0], c["idx"][2]) for c in oracle64.generate_contacts(rope, world).contacts()
+           if c["count"] == 4]
+    assert len(f64) >= 5
     one = rp.StepParams(dt=1e-3 / 16, substeps=1, iterations=4, linear_damping=1.0,
                         angular_damping=1.0)
+    lists = {}
     for s in STRATS:
         b = rp.Batch.create(proto, 1, s, pw)
         b.step(one)
-        pairs = [tuple(p) for p in b.read_self_contacts(0)]
-        assert pairs == expect, s
+        lists[s] = [tuple(int(v) for v in p) for p in b.read_self_contacts(0)]
         b.close()
+    assert lists[rp.Strategy.FUSED] == lists[rp.Strategy.MULTI_KERNEL] == lists[rp.Strategy.BATCHED]
+    from tests.helpers import segment_distance
+    x = rope.x[: rope.nP]
+    diff = set(lists[rp.Strategy.FUSED]) ^ set(f64)
+    assert len(diff) <= 2
+    for j, k in diff:
+        assert abs(segment_distance(x[j], x[j + 1], x[k], x[k + 1]) - 2 * 5e-3) < 1e-6, (j, k)
     # one full step vs the FP64 CPU
     cpu = rope.copy()
     oracle64.step(cpu, oparams(sp), world=world, ctx=Context())
@@ -263,6 +273,48 @@ def test_mixed_batch_equals_rods_alone(oracle64):
             alone.step_many(p, 5)
             assert np.array_equal(alone.download_positions(), mixed.positions_of(i, mx)), (i, s)
             alone.close()
+
+
+def test_batched_culls_and_levels_exact():
+    """The batched form's exact-safe shortcuts -- bounding-sphere prefilter of
+    self pairs, per-rod primitive culling, level-parallel self projection --
+    reproduce the plain kernel (the reference's serial order) bit for bit, on
+    tightly coiled rods whose turns start in contact (dozens of self contacts
+    per rod, several levels) among primitives of all kinds."""
+    from ropephysics_b200 import workloads as W
+    rng = np.random.default_rng(11)
+    rods, worlds = [], []
+    mat = rp.Material(1e8, 0.3, 1100.0, 5e-3)
+    for i in range(40):
+        n = int(rng.integers(40, 260))
+        pts = W.helix(n, 0.2 * n / 32, float(rng.uniform(0.03, 0.08)), pitch=1.97 * mat.radius)
+        r = rp.Rod.centerline(pts, mat)
+        r.b_rest_darboux[:] = 0.0
+        rods.append(r)
+        lo, hi = pts.min(0), pts.max(0)
+        prims = [W._random_primitive(rng, pts.mean(0), 0.5, lo, hi, clearance=-0.05)
+                 for _ in range(int(rng.integers(1, 5)))]
+        prims.append(rp.Primitive.plane((0, 0, lo[2] - 0.004), (0, 0, 1), 0.6))
+        worlds.append(rp.World(prims, self_collision=True, self_friction=0.4,
+                               hash_table_size=W.table_for(n) if i % 2 else 64))
+    p = rp.StepParams(dt=1.0 / 60, substeps=20, iterations=2)
+    out = {}
+    for s in (rp.Strategy.FUSED, rp.Strategy.BATCHED):
+        b = rp.Batch.create_mixed(rods, worlds, list(range(len(rods))), s)
+        pools = []
+        for _ in range(4):
+            b.step(p)
+            pools.append([b.read_self_contacts(i).tolist() for i in range(len(rods))])
+        out[s] = (b.download_positions(), b.read_contact_states(), pools, b.self_contact_overflow())
+        assert b.error_count() == 0
+        b.close()
+    a, c = out[rp.Strategy.FUSED], out[rp.Strategy.BATCHED]
+    assert np.array_equal(a[0], c[0])
+    assert np.array_equal(a[1], c[1])
+    assert a[2] == c[2]
+    assert a[3] == c[3]
+    assert max(len(pl) for step in a[2] for pl in step) >= 10
+    assert np.count_nonzero(a[1]) > 0
 
 
 def test_graph_replay_equals_direct_launches(oracle64):

@@ -25,6 +25,110 @@ OPAR = Params(dt=1e-3, substeps=8, iterations=1)
 STRATS = (rp.Strategy.MULTI_KERNEL, rp.Strategy.FUSED, rp.Strategy.BATCHED)
 
 
+def _ref_from(R, orod):
+    """A reference Rod handle holding the oracle rod's topology and state."""
+    h = R.from_rod(orod)
+    rr = R.export(h)
+    assert np.array_equal(rr.x, orod.x) and np.array_equal(rr.sComp, orod.sComp)
+    return h
+
+
+def _one_substep(p):
+    return rp.StepParams(dt=float(np.float32(p.dt)) / p.substeps, substeps=1, iterations=p.iterations,
+                         gravity=p.gravity, linear_damping=p.linear_damping,
+                         angular_damping=p.angular_damping)
+
+
+def test_self_pairs_bit_exact_vs_reference_gpu(reference_gpu, oracle64):
+    """Self-contact pair lists -- membership and order -- equal the reference
+    FP32 GPU kernel's from identical input state: the coiled rope restart of
+    gpu_cases.cpp:437-484 and tightly coiled rods with dozens of contacts,
+    at several hash-table sizes."""
+    R = reference_gpu
+    if not R.lib.refgpu_available():
+        pytest.skip("no device for the reference GPU path")
+    from tests.test_oracle import rope_restart_rod
+    from ropephysics_b200 import workloads as W
+    cases = []
+    rope, world, params, _ = rope_restart_rod(oracle64)
+    cases.append((rope, world))
+    rng = np.random.default_rng(5)
+    from oracle import World as OW, Primitive as OP
+    for table in (64, 256, 1024):
+        n = int(rng.integers(60, 250))
+        pts = W.helix(n, 0.2 * n / 32, float(rng.uniform(0.03, 0.08)), pitch=1.97 * 5e-3)
+        o = oracle64.centerline(pts, youngs=1e8, poisson=0.3, density=1100.0, radius=5e-3)
+        o.bRestD[:] = 0.0
+        cases.append((o, OW([OP.plane((0, 0, pts[:, 2].min() - 0.004), (0, 0, 1), 0.6)],
+                            self_collision=True, self_friction=0.4, hash_table_size=table)))
+    from tests.helpers import product_rod
+    total = 0
+    for orod, ow in cases:
+        h = _ref_from(R, orod)
+        wh = R.world(ow)
+        rb = R.lib.refgpu_create(h, 1, 0, wh)  # multi-kernel: pool in global memory
+        assert rb
+        one = _one_substep(rp.StepParams(dt=1e-3, substeps=16, iterations=2))
+        g = (ctypes.c_double * 3)(*one.gravity)
+        R.lib.refgpu_step(rb, one.dt, 1, one.iterations, g, 0.0, 0.0, 1, 1)
+        R.lib.refgpu_sync(rb)
+        expect = R.gpu_self_pairs(rb)
+        pw = rp.World([rp.Primitive(p.type, p.a, p.b, p.normal, p.half_extents, p.rotation,
+                                    p.radius, p.friction) for p in ow.primitives],
+                      self_collision=True, self_friction=ow.self_friction,
+                      hash_table_size=ow.hash_table_size)
+        proto = product_rod(orod)
+        for s in STRATS:
+            b = rp.Batch.create(proto, 1, s, pw)
+            b.step(one)
+            got = [tuple(int(v) for v in p) for p in b.read_self_contacts(0)]
+            assert got == expect, (s, ow.hash_table_size, len(got), len(expect))
+            b.close()
+        total += len(expect)
+        R.lib.refgpu_free(rb)
+        R.free(h)
+    assert total >= 40
+
+
+def test_contact_active_sets_vs_reference_gpu(reference_gpu, oracle64):
+    """World-contact active flags per (particle, primitive) equal the
+    reference FP32 GPU kernel's from identical input state, for all four
+    primitive types."""
+    R = reference_gpu
+    if not R.lib.refgpu_available():
+        pytest.skip("no device for the reference GPU path")
+    from oracle import World as OW, Primitive as OP
+    from tests.helpers import product_rod
+    n = 120
+    t = np.linspace(0, 4 * np.pi, n + 1)
+    pts = np.stack([0.1 * np.cos(t), 0.1 * np.sin(t), 0.3 + 0.01 * t], 1)
+    o = oracle64.centerline(pts, youngs=1e8, poisson=0.3, density=1100.0, radius=5e-3)
+    # each primitive overlaps the coil somewhere (the sphere touches the first
+    # particle, the capsule crosses the coil at y = -0.1, the box at y = 0.1)
+    prims = [OP.plane((0, 0, 0.3 - 0.003), (0, 0, 1), 0.5), OP.sphere((0.1165, 0.0, 0.3), 0.012, 0.3),
+             OP.capsule((-0.2, -0.1, 0.34), (0.2, -0.1, 0.34), 0.006, 0.4),
+             OP.box((0.0, 0.1, 0.36), (0.05, 0.004, 0.02), (0.9238795, 0, 0, 0.3826834), 0.6)]
+    ow = OW(prims)
+    h = _ref_from(R, o)
+    rb = R.lib.refgpu_create(h, 1, 0, R.world(ow))
+    one = _one_substep(rp.StepParams(dt=1e-3, substeps=8, iterations=1))
+    g = (ctypes.c_double * 3)(*one.gravity)
+    R.lib.refgpu_step(rb, one.dt, 1, 1, g, 0.0, 0.0, 1, 1)
+    R.lib.refgpu_sync(rb)
+    expect = R.gpu_contact_active(rb, 0, o.nP, len(prims))
+    pw = rp.World([rp.Primitive(p.type, p.a, p.b, p.normal, p.half_extents, p.rotation, p.radius,
+                                p.friction) for p in prims])
+    for s in STRATS:
+        b = rp.Batch.create(product_rod(o), 1, s, pw)
+        b.step(one)
+        got = (b.read_contact_states().reshape(o.nP, len(prims)) != 0).astype(np.int32)
+        assert np.array_equal(got, expect), s
+        b.close()
+    assert expect.sum(axis=0).min() >= 1  # every primitive type made contact
+    R.lib.refgpu_free(rb)
+    R.free(h)
+
+
 def _ref_rod(reference, n):
     h = reference.straight(n, 1.0, **REF_MAT)
     reference.lib.ref_rod_clamp(h, 0)
