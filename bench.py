@@ -113,8 +113,10 @@ def dist_setup(args):
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     return world, rank, local
 
 
@@ -123,7 +125,8 @@ def max_over_ranks(x: float, world: int) -> float:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -213,6 +216,83 @@ def cpu_reference_rate(wl, sample_rods: int, budget_s: float, threads: int):
     return rate, kind, sample, threads
 
 
+# ----------------------------------------------------------------------------- served stream
+
+
+def run_served(capacity: float, seconds: float, seed: int, load: float, budget_gb: float,
+               drain_s: float = 240.0):
+    """The served rollout stream: Poisson arrivals of requests with the
+    served-config shapes (1-1024 rods log-uniform, 32-512 segments, horizon
+    100-2000 steps, random features, grid materials), submitted in real time
+    to a continuous-batching server with an HBM admission budget. The spec's
+    200 requests/s offer far more work than one GPU executes, so the arrival
+    rate is set to `load` x the measured capacity and the spec's load factor is
+    reported beside it. Latency = completion - submission, per request."""
+    import threading
+
+    import ropephysics_b200 as rp
+    from ropephysics_b200 import workloads as W
+
+    params = rp.StepParams(dt=1.0 / 60, substeps=20, iterations=1)
+    rng = np.random.default_rng(seed)
+    probe = [W.served_request(np.random.default_rng(seed + 1000 + i)) for i in range(32)]
+    mean_work = float(np.mean([r.segment_substeps(params.substeps) for r in probe]))
+    spec_rate = 200.0
+    rate = max(0.05, load * capacity / mean_work)
+    import torch
+
+    torch.cuda.empty_cache()
+    free, _ = torch.cuda.mem_get_info()
+    # the arenas are the budget; leave room for the context and streams
+    budget = min(int(budget_gb * (1 << 30)), int(0.85 * free))
+    server = rp.Server(budget, params)
+    ids, errors = [], []
+
+    def submitter():
+        t_next = time.perf_counter()
+        t_end = t_next + seconds
+        while True:
+            t_next += rng.exponential(1.0 / rate)
+            if t_next > t_end:
+                break
+            req = W.served_request(rng)
+            delay = t_next - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            try:
+                ids.append(server.submit(req.rods, req.steps, req.worlds, [0] * len(req.rods),
+                                         req.drives, req.youngs_scale, req.friction_scale))
+            except rp.RopeError as e:
+                errors.append(str(e))
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    th.join()
+    try:
+        server.drain(drain_s)
+        drained = True
+    except rp.RopeError:
+        drained = False
+    st = server.stats()
+    infos = [server.info(i) for i in ids]
+    done = [i for i in infos if i["state"] == 2]
+    lat = sorted(i["done_s"] - i["submit_s"] for i in done)
+    work = sum(i["segment_substeps"] for i in done)
+    span = (max(i["done_s"] for i in done) - min(i["submit_s"] for i in infos)) if done else 0.0
+    server.close()
+    pct = lambda p: float(np.percentile(lat, p)) if lat else None
+    return {
+        "requests": len(ids), "completed": len(done), "drained": drained, "rejected": len(errors),
+        "p50_latency_s": pct(50), "p99_latency_s": pct(99), "mean_latency_s": float(np.mean(lat)) if lat else None,
+        "sustained": work / span if span > 0 else None, "unit": "segment-substeps/s",
+        "busy_s": st["busy_s"], "arrival_rate_req_s": rate, "window_s": seconds,
+        "load_vs_capacity": load, "spec_rate_req_s": spec_rate,
+        "spec_offered": spec_rate * mean_work, "spec_load_factor": spec_rate * mean_work / capacity,
+        "budget_bytes": st["budget_bytes"], "peak_resident_bytes": st["peak_resident_bytes"],
+        "steps_launched": st["steps_launched"],
+    }
+
+
 # ----------------------------------------------------------------------------- GPU arm
 
 
@@ -268,10 +348,16 @@ def run_ours(args):
         batch.synchronize()
     e2e_step()
     barrier(world_size)
-    t0 = time.perf_counter()
+    torch.cuda.synchronize()
+    # events on the batch's stream bracket the copies and the steps; every
+    # step ends in a host synchronize, so the span includes the host round trips
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
     for _ in range(e2e_steps):
         e2e_step()
-    e2e_s = max_over_ranks(time.perf_counter() - t0, world_size)
+    f1.record(stream)
+    f1.synchronize()
+    e2e_s = max_over_ranks(f0.elapsed_time(f1) / 1e3, world_size)
     e2e = seg_sub * e2e_steps * world_size / e2e_s
 
     # ---- plain one-rod-per-CTA step on the same batch (batched vs plain) ----
@@ -332,6 +418,10 @@ def run_ours(args):
                  "flops_per_segment_substep": FLOPS_PER_SEG_SUBSTEP.get(args.workload, 880.5)},
         "clocks": clk,
     }
+    if not args.no_served:
+        batch.close()
+        line["served"] = run_served(value / world_size, args.served_seconds, args.seed + 7 + rank,
+                                    args.served_load, args.served_budget_gb)
     if rank == 0 and world_size == 1 and not args.no_cpu:
         rate, kind, sample, threads = cpu_reference_rate(wl, args.cpu_rods, args.cpu_seconds,
                                                           os.cpu_count() or 1)
@@ -387,6 +477,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-rods", type=int, default=64)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--served-seconds", type=float, default=20.0)
+    ap.add_argument("--served-load", type=float, default=0.7)
+    ap.add_argument("--served-budget-gb", type=float, default=150.0)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

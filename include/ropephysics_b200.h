@@ -339,6 +339,75 @@ int64_t rp_batch_kernel_launches(const rp_batch* batch);
  * 0 in a correct run. -1 on a failed read. */
 int64_t rp_batch_error_count(rp_batch* batch);
 
+/* ------------------------------------------------------------------ serving */
+/* Continuous batching (no reference counterpart: the reference runs one
+ * Batch per caller). A server owns device arenas sized by an HBM budget and a
+ * worker thread. Requests -- sets of rods with a horizon in steps -- are
+ * admitted first-in first-out whenever their resident state fits the budget,
+ * join the rods already on the device, and advance together: every server
+ * step is ONE batched launch over all resident rods of all running requests.
+ * A request whose horizon is reached is read back and retired between steps,
+ * freeing its memory for the next admissions. Each rod's arithmetic is that
+ * of a batch holding it alone, so a request's result does not depend on what
+ * it shared the device with. All functions are thread-safe. */
+typedef struct rp_server rp_server;
+
+typedef struct rp_server_config {
+    uint64_t hbm_budget_bytes; /* resident-state budget for admission */
+    rp_step_params params;     /* shared by every request */
+    int32_t precision;         /* rp_precision flags */
+    int32_t max_steps_in_flight; /* launches queued ahead of completion checks (>= 1) */
+} rp_server_config;
+
+typedef struct rp_request {
+    const rp_rod_desc* const* rods;
+    int32_t num_rods;
+    int32_t steps;               /* horizon */
+    const rp_world* worlds;      /* may be NULL with num_worlds 0 */
+    int32_t num_worlds;
+    int32_t reserved;
+    const int32_t* world_of_rod; /* NULL: worlds[0] for every rod */
+    const rp_drive* drives;      /* one per rod, or NULL */
+    const float* youngs_scale;   /* one per rod, or NULL */
+    const float* friction_scale; /* one per rod, or NULL */
+} rp_request;
+
+enum { RP_REQUEST_QUEUED = 0, RP_REQUEST_RUNNING = 1, RP_REQUEST_DONE = 2 };
+
+typedef struct rp_request_info {
+    int32_t state;             /* RP_REQUEST_* */
+    int32_t num_rods;
+    int64_t num_particles;
+    int64_t resident_bytes;
+    int64_t segment_substeps;  /* work of the whole horizon */
+    double submit_s, admit_s, done_s; /* server clock, seconds */
+} rp_request_info;
+
+typedef struct rp_server_stats {
+    int64_t submitted, admitted, completed, queued, running;
+    int64_t steps_launched;
+    int64_t segment_substeps;  /* completed so far */
+    int64_t resident_bytes, peak_resident_bytes, budget_bytes;
+    double now_s;              /* server clock */
+    double busy_s;             /* time with at least one request running */
+} rp_server_stats;
+
+rp_status rp_server_create(const rp_server_config* config, rp_server** out);
+void rp_server_destroy(rp_server* server);
+/* Deep-copies the request. RP_ERR_BUDGET if it could never fit. */
+rp_status rp_server_submit(rp_server* server, const rp_request* request, uint64_t* id);
+rp_status rp_server_info(rp_server* server, uint64_t id, rp_request_info* out);
+/* Blocks until the request is done; RP_ERR_NOT_READY after timeout_s. */
+rp_status rp_server_wait(rp_server* server, uint64_t id, double timeout_s);
+/* Final positions of a finished request's rods, xyz floats, rods in request
+ * order. RP_ERR_NOT_READY while it runs. */
+rp_status rp_server_result(rp_server* server, uint64_t id, float* positions_xyz, int64_t capacity_floats);
+/* Forget a finished request (its result memory on the host). */
+rp_status rp_server_release(rp_server* server, uint64_t id);
+rp_status rp_server_get_stats(rp_server* server, rp_server_stats* out);
+/* Blocks until nothing is queued or running; RP_ERR_NOT_READY on timeout. */
+rp_status rp_server_drain(rp_server* server, double timeout_s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -446,6 +446,8 @@ class Reference:
         L.ref_step_many.argtypes = [C.POINTER(vp), C.POINTER(vp), C.c_int, C.c_double, C.c_int,
                                     C.c_int, d3, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int]
         L.ref_generate_contacts.argtypes = [vp, vp, C.POINTER(C.c_int), d3, d3, d3, C.c_int]
+        L.ref_hold_many.argtypes = [C.POINTER(vp), C.POINTER(vp), C.c_int, C.c_double, C.c_int, C.c_int,
+                                    d3, C.c_int, C.c_int, C.c_int, d3, C.POINTER(C.c_int)]
         L.ref_contacts.argtypes = [vp, C.POINTER(C.c_int), d3, d3, d3, C.c_int]
         self.gpu = gpu
         if gpu:
@@ -493,6 +495,22 @@ class Reference:
         return self.lib.ref_rod_centerline(pts.ctypes.data_as(C.POINTER(C.c_double)), len(pts),
                                            youngs, poisson, density, radius,
                                            Oracle._d3(frame_seed), float(twist_per_length))
+
+    def hanging(self, legRatio, youngs, length=1.0, segments=100, bar_radius=0.05, bar_height=0.8):
+        """The cable of the reference's cable task (apps/cable_hanging.cpp:18-47)."""
+        return self.lib.ref_rod_hanging(length, segments, bar_radius, bar_height, legRatio, youngs)
+
+    def hold_many(self, handles, world_handles, p: Params, steps, interval, threads):
+        """Reference HangOutcome verdicts (max rise of particle 0, held) per rod."""
+        n = len(handles)
+        H = (C.c_void_p * n)(*handles)
+        W = (C.c_void_p * n)(*world_handles)
+        rise = np.zeros(n)
+        held = np.zeros(n, np.int32)
+        self.lib.ref_hold_many(H, W, n, p.dt, p.substeps, p.iterations, Oracle._d3(p.gravity), steps,
+                               interval, threads, rise.ctypes.data_as(C.POINTER(C.c_double)),
+                               held.ctypes.data_as(C.POINTER(C.c_int)))
+        return rise, held.astype(bool)
 
     def from_rod(self, rod: Rod):
         """A reference Rod handle holding exactly `rod`'s arrays."""

@@ -360,6 +360,40 @@ double ref_step_many(void** rods, void** worlds, int numRods, double dt, int sub
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
+// Hold/slide verdicts of many cables on the reference's FP64 solver, in its
+// colour order, observed with its own HangOutcome (cable_hanging.h:68-77):
+// the short end (particle 0) is sampled every `interval` steps and at the
+// last step; held <=> max rise <= 0.05 m. Rods spread over `threads`.
+void ref_hold_many(void** rods, void** worlds, int numRods, double dt, int substeps, int iterations,
+                   const double* g, int steps, int interval, int threads, double* maxRise, int* held) {
+    SolverParams base = params(dt, substeps, iterations, g, 0.0, 0.0, 1);
+    auto work = [&](int b, int e) {
+        for (int r = b; r < e; ++r) {
+            auto* h = static_cast<RodHandle*>(rods[r]);
+            h->sc = colorStretchConstraints(h->rod);
+            h->bc = colorBendConstraints(h->rod);
+            SolverParams p = base;
+            p.stretchColoring = &h->sc;
+            p.bendColoring = &h->bc;
+            apps::HangOutcome outcome(h->rod.state.x.front().z);
+            for (int s = 1; s <= steps; ++s) {
+                step(h->rod, p, static_cast<WorldHandle*>(worlds[r])->world, h->ctx);
+                if (s % interval == 0 || s == steps) outcome.observe(h->rod.state.x.front().z);
+            }
+            maxRise[r] = outcome.maxRise;
+            held[r] = outcome.held() ? 1 : 0;
+        }
+    };
+    threads = std::max(1, std::min(threads, numRods));
+    std::vector<std::thread> pool;
+    const int per = (numRods + threads - 1) / threads;
+    for (int t = 0; t < threads; ++t) {
+        const int b = t * per, e = std::min(numRods, b + per);
+        if (b < e) pool.emplace_back(work, b, e);
+    }
+    for (auto& th : pool) th.join();
+}
+
 // The rod's current contact list (the one the last substep used), as
 // idx[4], weight[4], normal[3], offset, friction, lambdaN per contact.
 int ref_contacts(void* hp, int* idx, double* weight, double* normal, double* offset, int cap) {

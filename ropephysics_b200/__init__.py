@@ -24,8 +24,8 @@ import numpy as np
 from . import _abi
 
 __all__ = ["RopeError", "Strategy", "Precision", "ContactState", "Material", "Primitive", "World",
-           "StepParams", "Drive", "Rod", "Batch", "cuda_available", "device_name", "diagnostic",
-           "max_fused_segments", "coloring", "self_collision_index_gap", "lib"]
+           "StepParams", "Drive", "Rod", "Batch", "Server", "cuda_available", "device_name",
+           "diagnostic", "max_fused_segments", "coloring", "self_collision_index_gap", "lib"]
 
 
 def lib():
@@ -574,3 +574,93 @@ class Batch:
 
     def num_segments(self, rod_index: int = 0) -> int:
         return lib().rp_batch_num_segments(self._h, rod_index)
+
+
+class Server:
+    """Continuous-batching server (rp_server_*): requests of rods with a
+    horizon, admitted by an HBM budget, stepped together in one launch per
+    step, retired when done."""
+
+    def __init__(self, budget_bytes: int, params: StepParams, precision: int = 0):
+        cfg = _abi.ServerConfig()
+        cfg.hbm_budget_bytes = int(budget_bytes)
+        cfg.params = params.to_c()
+        cfg.precision = int(precision)
+        cfg.max_steps_in_flight = 1
+        h = C.c_void_p()
+        _check(lib().rp_server_create(C.byref(cfg), C.byref(h)))
+        self._h = h
+        self._keep = {}
+
+    def close(self):
+        if self._h:
+            lib().rp_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, rods: Sequence[Rod], steps: int, worlds: Sequence[World] = (),
+               world_of_rod=None, drives: Optional[Sequence[Drive]] = None, youngs_scale=None,
+               friction_scale=None) -> int:
+        req = _abi.Request()
+        descs = (C.POINTER(_abi.RodDesc) * len(rods))(*[C.pointer(r.desc) for r in rods])
+        req.rods = descs
+        req.num_rods = len(rods)
+        req.steps = int(steps)
+        cw = [w.to_c() for w in worlds]
+        warr = (_abi.World * max(1, len(cw)))(*cw) if cw else None
+        req.worlds = warr
+        req.num_worlds = len(cw)
+        keep = [descs, cw, warr, rods]
+        if world_of_rod is not None:
+            wor = np.ascontiguousarray(world_of_rod, np.int32)
+            req.world_of_rod = wor.ctypes.data_as(_I32)
+            keep.append(wor)
+        if drives is not None:
+            arr = (_abi.Drive * len(drives))()
+            for i, d in enumerate(drives):
+                arr[i].particle = d.particle
+                arr[i].axis[:] = [float(v) for v in d.axis]
+                arr[i].amplitude = d.amplitude
+                arr[i].frequency = d.frequency
+                arr[i].phase = d.phase
+            req.drives = arr
+            keep.append(arr)
+        FP = C.POINTER(C.c_float)
+        for name, val in (("youngs_scale", youngs_scale), ("friction_scale", friction_scale)):
+            if val is not None:
+                a = np.ascontiguousarray(val, np.float32)
+                setattr(req, name, a.ctypes.data_as(FP))
+                keep.append(a)
+        rid = C.c_uint64()
+        _check(lib().rp_server_submit(self._h, C.byref(req), C.byref(rid)))
+        return rid.value
+
+    def info(self, rid: int) -> dict:
+        i = _abi.RequestInfo()
+        _check(lib().rp_server_info(self._h, rid, C.byref(i)))
+        return {f: getattr(i, f) for f, _ in _abi.RequestInfo._fields_}
+
+    def wait(self, rid: int, timeout: float = 600.0):
+        _check(lib().rp_server_wait(self._h, rid, float(timeout)))
+
+    def result(self, rid: int) -> np.ndarray:
+        n = self.info(rid)["num_particles"]
+        out = np.zeros((n, 3), np.float32)
+        _check(lib().rp_server_result(self._h, rid, out.ctypes.data_as(C.POINTER(C.c_float)), out.size))
+        return out
+
+    def release(self, rid: int):
+        _check(lib().rp_server_release(self._h, rid))
+
+    def stats(self) -> dict:
+        s = _abi.ServerStats()
+        _check(lib().rp_server_get_stats(self._h, C.byref(s)))
+        return {f: getattr(s, f) for f, _ in _abi.ServerStats._fields_}
+
+    def drain(self, timeout: float = 600.0):
+        _check(lib().rp_server_drain(self._h, float(timeout)))

@@ -57,6 +57,29 @@ class Drive(C.Structure):
                 ("frequency", f32), ("phase", f32)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("params", StepParams), ("precision", i32),
+                ("max_steps_in_flight", i32)]
+
+
+class Request(C.Structure):
+    _fields_ = [("rods", P(P(RodDesc))), ("num_rods", i32), ("steps", i32), ("worlds", P(World)),
+                ("num_worlds", i32), ("reserved", i32), ("world_of_rod", P(i32)), ("drives", P(Drive)),
+                ("youngs_scale", P(f32)), ("friction_scale", P(f32))]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("state", i32), ("num_rods", i32), ("num_particles", i64), ("resident_bytes", i64),
+                ("segment_substeps", i64), ("submit_s", f64), ("admit_s", f64), ("done_s", f64)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", i64), ("admitted", i64), ("completed", i64), ("queued", i64),
+                ("running", i64), ("steps_launched", i64), ("segment_substeps", i64),
+                ("resident_bytes", i64), ("peak_resident_bytes", i64), ("budget_bytes", i64),
+                ("now_s", f64), ("busy_s", f64)]
+
+
 vp = C.c_void_p
 pp = P(vp)
 
@@ -118,6 +141,15 @@ SIGNATURES = {
     "rp_batch_self_contact_overflow": (i64, [vp]),
     "rp_batch_kernel_launches": (i64, [vp]),
     "rp_batch_error_count": (i64, [vp]),
+    "rp_server_create": (i32, [P(ServerConfig), pp]),
+    "rp_server_destroy": (None, [vp]),
+    "rp_server_submit": (i32, [vp, P(Request), P(C.c_uint64)]),
+    "rp_server_info": (i32, [vp, C.c_uint64, P(RequestInfo)]),
+    "rp_server_wait": (i32, [vp, C.c_uint64, f64]),
+    "rp_server_result": (i32, [vp, C.c_uint64, P(f32), i64]),
+    "rp_server_release": (i32, [vp, C.c_uint64]),
+    "rp_server_get_stats": (i32, [vp, P(ServerStats)]),
+    "rp_server_drain": (i32, [vp, f64]),
 }
 
 _lib = None

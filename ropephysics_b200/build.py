@@ -29,7 +29,7 @@ NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-r
 CXX_FLAGS = ["-std=c++17", "-O3", "-fPIC", "-Wall", "-Wextra", "-Wno-unused-parameter"]
 
 CU_SOURCES = ["rp_plain.cu", "rp_batched.cu"]
-CPP_SOURCES = ["rp_rod.cpp", "rp_batch.cpp"]
+CPP_SOURCES = ["rp_rod.cpp", "rp_hostutil.cpp", "rp_batch.cpp", "rp_server.cpp"]
 HEADERS = ["rp_internal.h", "rp_layout.h", "rp_launch.h", "rp_math.cuh", "rp_step_common.cuh",
            "rp_host.h"]
 

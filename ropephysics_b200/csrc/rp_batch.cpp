@@ -56,10 +56,6 @@ struct Tune {
     int pairsPerThread = 1;  // team threads ~ ceil(nSt / 2 / pairsPerThread), rounded to 32
 };
 
-float4 f4(double a, double b, double c, double d = 0.0) {
-    return make_float4(float(a), float(b), float(c), float(d));
-}
-
 }  // namespace
 
 struct rp_batch {
@@ -146,109 +142,13 @@ struct rp_batch {
 
 namespace {
 
-bool deviceUsable(std::string* why) {
-    int n = 0;
-    const cudaError_t e = cudaGetDeviceCount(&n);
-    if (e != cudaSuccess || n == 0) {
-        if (why) {
-            int rt = 0, dr = 0;
-            cudaRuntimeGetVersion(&rt);
-            cudaDriverGetVersion(&dr);
-            *why = std::string("no usable CUDA device: error ") + std::to_string(int(e)) + " (" +
-                   cudaGetErrorString(e) + "); runtime CUDA " + std::to_string(rt / 1000) + "." +
-                   std::to_string((rt % 1000) / 10) + ", driver supports CUDA " +
-                   std::to_string(dr / 1000) + "." + std::to_string((dr % 1000) / 10);
-        }
-        cudaGetLastError();
-        return false;
-    }
-    return true;
-}
-
-size_t optinSmem(int device) {
-    int v = 0;
-    if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess) {
-        cudaGetLastError();
-        return 48 * 1024;
-    }
-    return size_t(v);
-}
-
-DPrim toDPrim(const rp_primitive& p) {
-    DPrim d{};
-    d.ax = float(p.a[0]);
-    d.ay = float(p.a[1]);
-    d.az = float(p.a[2]);
-    d.radius = float(p.radius);
-    d.bx = float(p.b[0]);
-    d.by = float(p.b[1]);
-    d.bz = float(p.b[2]);
-    d.friction = float(p.friction);
-    d.nx = float(p.normal[0]);
-    d.ny = float(p.normal[1]);
-    d.nz = float(p.normal[2]);
-    d.typef = float(p.type);
-    d.hx = float(p.half_extents[0]);
-    d.hy = float(p.half_extents[1]);
-    d.hz = float(p.half_extents[2]);
-    d.qw = float(p.rotation[0]);
-    d.qx = float(p.rotation[1]);
-    d.qy = float(p.rotation[2]);
-    d.qz = float(p.rotation[3]);
-    return d;
-}
-
-std::string validateWorld(const rp_world& w) {
-    if (w.num_primitives < 0 || (w.num_primitives > 0 && !w.primitives))
-        return "world has primitives but a NULL array";
-    if (w.num_primitives > 64) return "at most 64 primitives per world";
-    for (int k = 0; k < w.num_primitives; ++k) {
-        const rp_primitive& p = w.primitives[k];
-        if (p.type < 0 || p.type > 3) return "primitive type must be 0..3";
-        if ((p.type == 1 || p.type == 2) && !(p.radius >= 0)) return "negative primitive radius";
-    }
-    if (w.self_collision && (w.hash_table_size < 1 || w.hash_table_size > (1 << 20)))
-        return "self-collision needs 1 <= hash_table_size <= 2^20";
-    return "";
-}
-
-// Chain topology: stretch k = (k, k+1, frame k); bends 0..nSt-2 = (k, k+1);
-// any further bends involve a ghost frame (index >= nSt).
-int isChain(const rp_rod_desc* d) {
-    if (d->num_particles != d->num_stretch + 1) return 0;
-    for (int k = 0; k < d->num_stretch; ++k)
-        if (d->s_p0[k] != k || d->s_p1[k] != k + 1 || d->s_seg[k] != k) return 0;
-    if (d->num_bend < d->num_stretch - 1) return 0;
-    for (int k = 0; k < d->num_stretch - 1; ++k)
-        if (d->b_a[k] != k || d->b_b[k] != k + 1) return 0;
-    for (int k = d->num_stretch - 1; k < d->num_bend; ++k)
-        if (d->b_a[k] < d->num_stretch && d->b_b[k] < d->num_stretch) return 0;
-    return 1;
-}
-
-// Per-rod state upload helpers: double descriptor -> float4 rows.
-void packParticles(const rp_rod_desc* d, float4* x, float4* v, float4* f, float4* k) {
-    for (int i = 0; i < d->num_particles; ++i) {
-        if (x) x[i] = f4(d->x[3 * i], d->x[3 * i + 1], d->x[3 * i + 2]);
-        if (v) v[i] = d->v ? f4(d->v[3 * i], d->v[3 * i + 1], d->v[3 * i + 2]) : f4(0, 0, 0);
-        if (f)
-            f[i] = d->ext_force ? f4(d->ext_force[3 * i], d->ext_force[3 * i + 1], d->ext_force[3 * i + 2])
-                                : f4(0, 0, 0);
-        if (k)
-            k[i] = d->kin_velocity
-                       ? f4(d->kin_velocity[3 * i], d->kin_velocity[3 * i + 1], d->kin_velocity[3 * i + 2])
-                       : f4(0, 0, 0);
-    }
-}
-void packFrames(const rp_rod_desc* d, float4* q, float4* w, float4* t) {
-    for (int j = 0; j < d->num_frames; ++j) {
-        if (q) q[j] = f4(d->q[4 * j], d->q[4 * j + 1], d->q[4 * j + 2], d->q[4 * j + 3]);
-        if (w) w[j] = d->omega ? f4(d->omega[3 * j], d->omega[3 * j + 1], d->omega[3 * j + 2]) : f4(0, 0, 0);
-        if (t)
-            t[j] = d->ext_torque ? f4(d->ext_torque[3 * j], d->ext_torque[3 * j + 1], d->ext_torque[3 * j + 2])
-                                 : f4(0, 0, 0);
-    }
-}
+using rpx::deviceUsable;
+using rpx::isChain;
+using rpx::optinSmem;
+using rpx::packFrames;
+using rpx::packParticles;
+using rpx::toDPrim;
+using rpx::validateWorld;
 
 bool sameTopology(const rp_batch* b, int r, const rp_rod_desc* d) {
     return d && d->num_particles == b->tmplNP[r] && d->num_frames == b->tmplNS[r];
@@ -315,51 +215,32 @@ static rp_status createImpl(const rp_rod_desc* const* rods, int numRods, const r
     std::vector<float4> tInvInertia, tInertia, tSComp, tBComp, tBRestD;
     std::vector<int32_t> tSP0, tSP1, tSSeg, tBA, tBB, tOrder, tColorStart;
     for (const rp_rod_desc* d : tdesc) {
-        DTemplate T{};
-        T.nP = d->num_particles;
-        T.nS = d->num_frames;
-        T.nSt = d->num_stretch;
-        T.nB = d->num_bend;
+        rpx::TemplateHost th;
+        rpx::makeTemplate(d, th);
+        DTemplate T = th.T;
         T.pOff = int(tInvMass.size());
         T.sOff = int(tInvInertia.size());
         T.stOff = int(tSP0.size());
         T.bOff = int(tBA.size());
-        for (int i = 0; i < T.nP; ++i) tInvMass.push_back(float(d->inv_mass[i]));
-        std::vector<char> fixed(T.nS, 0);
-        for (int j = 0; j < T.nS; ++j) {
-            const double* iI = d->inv_inertia + 3 * j;
-            tInvInertia.push_back(f4(iI[0], iI[1], iI[2]));
-            tInertia.push_back(f4(d->inertia[3 * j], d->inertia[3 * j + 1], d->inertia[3 * j + 2]));
-            fixed[j] = (iI[0] * iI[0] + iI[1] * iI[1] + iI[2] * iI[2]) == 0.0;
-        }
-        b->fixedFrame.push_back(fixed);
-        for (int k = 0; k < T.nSt; ++k) {
-            tSP0.push_back(d->s_p0[k]);
-            tSP1.push_back(d->s_p1[k]);
-            tSSeg.push_back(d->s_seg[k]);
-            tSComp.push_back(f4(d->s_compliance[3 * k], d->s_compliance[3 * k + 1],
-                                d->s_compliance[3 * k + 2], d->s_rest[k]));
-        }
-        for (int k = 0; k < T.nB; ++k) {
-            tBA.push_back(d->b_a[k]);
-            tBB.push_back(d->b_b[k]);
-            tBComp.push_back(f4(d->b_compliance[3 * k], d->b_compliance[3 * k + 1],
-                                d->b_compliance[3 * k + 2], d->b_rest[k]));
-            tBRestD.push_back(f4(d->b_rest_darboux[3 * k], d->b_rest_darboux[3 * k + 1],
-                                 d->b_rest_darboux[3 * k + 2]));
-        }
-        std::vector<int> order, cs;
-        T.sColors = rpx::colorRod(d, false, order, cs);
-        T.sOrderOff = int(tOrder.size());
-        tOrder.insert(tOrder.end(), order.begin(), order.end());
-        T.sColorOff = int(tColorStart.size());
-        tColorStart.insert(tColorStart.end(), cs.begin(), cs.end());
-        T.bColors = rpx::colorRod(d, true, order, cs);
-        T.bOrderOff = int(tOrder.size());
-        tOrder.insert(tOrder.end(), order.begin(), order.end());
-        T.bColorOff = int(tColorStart.size());
-        tColorStart.insert(tColorStart.end(), cs.begin(), cs.end());
-        T.chain = isChain(d);
+        T.sOrderOff += int(tOrder.size());
+        T.bOrderOff += int(tOrder.size());
+        T.sColorOff += int(tColorStart.size());
+        T.bColorOff += int(tColorStart.size());
+        auto app = [](auto& dst, const auto& src) { dst.insert(dst.end(), src.begin(), src.end()); };
+        app(tInvMass, th.invMass);
+        app(tInvInertia, th.invInertia);
+        app(tInertia, th.inertia);
+        app(tSP0, th.sP0);
+        app(tSP1, th.sP1);
+        app(tSSeg, th.sSeg);
+        app(tSComp, th.sComp);
+        app(tBA, th.bA);
+        app(tBB, th.bB);
+        app(tBComp, th.bComp);
+        app(tBRestD, th.bRestD);
+        app(tOrder, th.order);
+        app(tColorStart, th.colorStart);
+        b->fixedFrame.push_back(th.fixed);
         b->sColorsMax = std::max(b->sColorsMax, T.sColors);
         b->bColorsMax = std::max(b->bColorsMax, T.bColors);
         b->tmpls.push_back(T);
@@ -571,50 +452,14 @@ static rp_status createImpl(const rp_rod_desc* const* rods, int numRods, const r
 
 namespace {
 
-// Team size for a rod of nSt segments: enough threads that each handles about
-// `pairsPerThread` constraints of a colour, rounded to whole warps, 32..256.
-int teamThreads(int nSt, int pairsPerThread) {
-    int t = (nSt / 2 + pairsPerThread - 1) / pairsPerThread;
-    t = (t + 31) / 32 * 32;
-    return std::max(32, std::min(256, t));
-}
-
 rp_status buildBatchedPlan(rp_batch* b) {
     // Length-sorted work order: longest first, so the tail of the persistent
     // queue is short rods and the SMs finish together.
-    std::vector<int32_t> order(b->numRods);
-    for (int r = 0; r < b->numRods; ++r) order[r] = r;
-    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-        const int nx = b->tmpls[b->rods[x].tmpl].nSt, ny = b->tmpls[b->rods[y].tmpl].nSt;
-        return nx > ny;
-    });
+    std::vector<int32_t> ids(b->numRods), order;
+    for (int r = 0; r < b->numRods; ++r) ids[r] = r;
     const int cta = b->tune.ctaThreads;
-    b->groups.clear();
-    size_t maxSmem = 0;
-    int i = 0;
-    while (i < b->numRods) {
-        const DRod& R0 = b->rods[order[i]];
-        const int team = std::min(cta, teamThreads(b->tmpls[R0.tmpl].nSt, b->tune.pairsPerThread));
-        const int perCta = cta / team;
-        int cnt = 0;
-        size_t smem = 0;
-        while (i + cnt < b->numRods && cnt < perCta) {
-            const DRod& R = b->rods[order[i + cnt]];
-            const DTemplate& T = b->tmpls[R.tmpl];
-            if (std::min(cta, teamThreads(T.nSt, b->tune.pairsPerThread)) != team) break;
-            const rp::RodLayout L =
-                rp::rodLayout(T.nP, T.nS, T.nSt, T.nB, R.numPrims, R.selfCollision, R.hashTableSize,
-                              R.selfCapacity, 1, (b->precision & RP_PRECISION_COMPENSATED) ? 1 : 0);
-            smem += size_t(L.bytes);
-            ++cnt;
-        }
-        b->groups.push_back(i);
-        b->groups.push_back(cnt);
-        b->groups.push_back(team);
-        b->groups.push_back(int32_t(smem));
-        maxSmem = std::max(maxSmem, smem);
-        i += cnt;
-    }
+    const size_t maxSmem = rpx::planGroups(ids, b->rods.data(), b->tmpls.data(), cta, b->tune.pairsPerThread,
+                                           (b->precision & RP_PRECISION_COMPENSATED) != 0, order, b->groups);
     b->numGroups = int(b->groups.size() / 4);
     const size_t optin = optinSmem(b->device);
     if (maxSmem + 1024 > optin)  // the kernel also has a few bytes of static shared memory

@@ -1,10 +1,13 @@
 // rp_host.h -- host-side internals shared by the C ABI translation units.
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <string>
 #include <vector>
 
 #include "ropephysics_b200.h"
+#include "rp_internal.h"
 
 // Host rod: the reference Rod's arrays (src/core/rod.h:49-121) in double.
 struct rp_rod {
@@ -30,5 +33,27 @@ int colorGreedy(int count, const std::vector<int>& start, const std::vector<int>
                 std::vector<int>& order, std::vector<int>& colorStart);
 int colorRod(const rp_rod_desc* d, bool bend, std::vector<int>& order, std::vector<int>& colorStart);
 int selfGap(const rp_rod_desc* d, int selfSkip);
+
+// ---- rp_hostutil.cpp ----
+bool deviceUsable(std::string* why);
+size_t optinSmem(int device);
+rp::DPrim toDPrim(const rp_primitive& p);
+std::string validateWorld(const rp_world& w);
+int isChain(const rp_rod_desc* d);
+void packParticles(const rp_rod_desc* d, float4* x, float4* v, float4* f, float4* k);
+void packFrames(const rp_rod_desc* d, float4* q, float4* w, float4* t);
+
+struct TemplateHost {
+    rp::DTemplate T;
+    std::vector<float> invMass;
+    std::vector<float4> invInertia, inertia, sComp, bComp, bRestD;
+    std::vector<int32_t> sP0, sP1, sSeg, bA, bB, order, colorStart;
+    std::vector<char> fixed;
+};
+void makeTemplate(const rp_rod_desc* d, TemplateHost& out);
+int teamThreads(int nSt, int pairsPerThread);
+size_t planGroups(const std::vector<int32_t>& rodIds, const rp::DRod* rods, const rp::DTemplate* tmpls,
+                  int cta, int pairsPerThread, bool comp, std::vector<int32_t>& order,
+                  std::vector<int32_t>& groups);
 
 }  // namespace rpx

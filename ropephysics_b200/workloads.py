@@ -169,6 +169,54 @@ def uneven(num_rods: int = 16384, seed: int = 0, min_seg: int = 16, max_seg: int
                     info=dict(seed=seed, hash_table_size=hash_table_size or "2n, pow2, 64..1024"))
 
 
+@dataclass
+class ServedRequest:
+    rods: List[Rod]
+    steps: int
+    worlds: List[World]
+    drives: Optional[List[Drive]]
+    youngs_scale: np.ndarray
+    friction_scale: np.ndarray
+    features: dict
+
+    def segment_substeps(self, substeps: int) -> int:
+        return int(sum(r.num_stretch for r in self.rods)) * substeps * self.steps
+
+
+def served_request(rng, max_rods: int = 1024, min_seg: int = 32, max_seg: int = 512,
+                   min_steps: int = 100, max_steps: int = 2000) -> ServedRequest:
+    """One request of the served stream: 1..max_rods rods (log-uniform) of one
+    shape with U{min_seg..max_seg} segments hanging from a pinned top, a
+    horizon U{min_steps..max_steps}, each feature -- floor, primitives, driven
+    top, self-collision -- present with probability 1/2, and per-rod material
+    as in the grid (E x U(0.4, 4), mu x U(0.6, 1.4))."""
+    count = int(round(math.exp(rng.uniform(0.0, math.log(max_rods)))))
+    count = max(1, min(max_rods, count))
+    n = int(rng.integers(min_seg, max_seg + 1))
+    steps = int(rng.integers(min_steps, max_steps + 1))
+    feats = {k: bool(rng.random() < 0.5) for k in ("floor", "primitives", "driven", "self")}
+    length = n / 64.0
+    rod = Rod.straight(n, length, GRID_MATERIAL, origin=(0.0, 0.0, 0.0), direction=(0.0, 0.0, -1.0))
+    rod.pin_particle(0)
+    mu = 0.5
+    prims = []
+    if feats["floor"]:
+        prims.append(Primitive.plane((0.0, 0.0, -length - 0.05), (0.0, 0.0, 1.0), mu))
+    if feats["primitives"]:
+        lo, hi = np.array([0.0, 0.0, -length]), np.array([0.0, 0.0, 0.0])
+        for _ in range(int(rng.integers(1, 5))):
+            prims.append(_random_primitive(rng, (0.0, 0.0, -length / 2), mu, lo, hi))
+    world = World(prims, self_collision=feats["self"], self_friction=mu, hash_table_size=table_for(n))
+    drives = None
+    if feats["driven"]:
+        drives = [Drive(0, (0.0, 0.0, 1.0), float(a), float(f), float(p))
+                  for a, f, p in zip(rng.uniform(0.0, 0.1, count), rng.uniform(0.5, 2.0, count),
+                                     rng.uniform(0.0, 2 * math.pi, count))]
+    ys = rng.uniform(0.4, 4.0, count).astype(np.float32)
+    fs = rng.uniform(0.6, 1.4, count).astype(np.float32)
+    return ServedRequest([rod] * count, steps, [world], drives, ys, fs, feats)
+
+
 def hanging_cable_points(leg_ratio: float, length=1.2, segments=120, bar_radius=0.02,
                          bar_height=0.8, cable_radius=0.004):
     """Drape over a horizontal bar (the geometry of the reference's cable
