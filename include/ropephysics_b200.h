@@ -247,6 +247,21 @@ rp_status rp_batch_step(rp_batch* batch, const rp_step_params* params);
 /* `steps` steps; when graphs are enabled (rp_batch_set_graph) the sequence is
  * replayed from a captured CUDA graph. */
 rp_status rp_batch_step_many(rp_batch* batch, const rp_step_params* params, int32_t steps);
+/* No reference counterpart. One step of an RP_STRATEGY_BATCHED batch, the
+ * same kernel and the same results as rp_batch_step, but the step's scratch
+ * (work-queue counters, start-of-substep frames, world-contact slots,
+ * self-contact pool) is carved from a fixed static device array of
+ * RP_STATIC_SCRATCH_BYTES instead of the batch's own buffers, and the call
+ * allocates no device memory. Needs: 256 + 16 x frames + 32 x contact slots
+ * (+ 64 x self-contact pool entries), each section rounded up to 256 bytes;
+ * a larger batch is rejected with RP_ERR_INVALID. The batch's device must be
+ * current. The first call on a device looks up the array's address, once;
+ * make that first call before any stream capture. The queue counters are
+ * cleared on the batch's stream before each launch; nothing else needs to
+ * start at zero. The array is shared by every call on the device: calls that
+ * overlap in time (other streams, threads or batches) race on it. */
+#define RP_STATIC_SCRATCH_BYTES (32u << 20)
+rp_status rp_batch_step_static_scratch(rp_batch* batch, const rp_step_params* params);
 /* reference: Batch::synchronize, gpu_solver.h:86 */
 rp_status rp_batch_synchronize(rp_batch* batch);
 /* Run the batch on a caller-owned cudaStream_t (NULL = the library's own). */

@@ -107,6 +107,7 @@ SIGNATURES = {
     "rp_batch_destroy": (None, [vp]),
     "rp_batch_step": (i32, [vp, P(StepParams)]),
     "rp_batch_step_many": (i32, [vp, P(StepParams), i32]),
+    "rp_batch_step_static_scratch": (i32, [vp, P(StepParams)]),
     "rp_batch_synchronize": (i32, [vp]),
     "rp_batch_set_stream": (i32, [vp, vp]),
     "rp_batch_set_precision": (i32, [vp, i32]),

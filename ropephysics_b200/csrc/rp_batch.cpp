@@ -632,6 +632,54 @@ rp_status rp_batch_step(rp_batch* b, const rp_step_params* p) {
     return launchStep(b, p);
 }
 
+rp_status rp_batch_step_static_scratch(rp_batch* b, const rp_step_params* p) {
+    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
+    rp_status st = validateParams(p);
+    if (st != RP_OK) return st;
+    if (b->strategy != RP_STRATEGY_BATCHED)
+        return fail(RP_ERR_INVALID, "rp_batch_step_static_scratch needs an RP_STRATEGY_BATCHED batch");
+    int dev = -1;
+    RP_CUDA(cudaGetDevice(&dev));
+    if (dev != b->device)
+        return fail(RP_ERR_INVALID, "the batch's device (" + std::to_string(b->device) + ") must be current");
+    // scratch sections, 256-byte aligned: work-queue counters, start-of-substep
+    // frames, world-contact slots, self-contact pool
+    auto up = [](size_t n) { return (n + 255) & ~size_t(255); };
+    const size_t qPrevAt = 256;
+    const size_t slotsAt = qPrevAt + up(size_t(b->totalS) * sizeof(float4));
+    const size_t poolAt = slotsAt + up(size_t(b->totalSlots) * sizeof(rp::DSlot));
+    const size_t need = poolAt + (b->anySelf ? up(size_t(b->totalPool) * sizeof(rp::DSelf)) : 0);
+    void* base = nullptr;
+    size_t have = 0;
+    const cudaError_t e = rp::staticScratch(&base, &have);
+    if (e != cudaSuccess)
+        return fail(RP_ERR_CUDA, std::string("static scratch set-up failed: ") + cudaGetErrorString(e));
+    if (need > have)
+        return fail(RP_ERR_INVALID, "this batch's step needs " + std::to_string(need) +
+                                        " bytes of scratch; the static scratch holds " + std::to_string(have) +
+                                        " (RP_STATIC_SCRATCH_BYTES); use rp_batch_step");
+    unsigned char* s = static_cast<unsigned char*>(base);
+    DArgs A = b->a;
+    fillStepArgs(b, p, A);
+    A.gqPrev = reinterpret_cast<float4*>(s + qPrevAt);
+    A.gSlots = reinterpret_cast<rp::DSlot*>(s + slotsAt);
+    A.gPool = b->anySelf ? reinterpret_cast<rp::DSelf*>(s + poolAt) : nullptr;
+    rp::BatchedPlan plan;
+    plan.groups = b->dGroups;
+    plan.numGroups = b->numGroups;
+    plan.queue = reinterpret_cast<int32_t*>(s);
+    plan.blocks = b->batchedBlocks;
+    plan.threads = b->batchedThreads;
+    plan.smemBytes = b->batchedSmem;
+    // the two work-queue counters must be zero at launch; everything else is
+    // written before it is read within the step
+    RP_CUDA(cudaMemsetAsync(plan.queue, 0, 2 * sizeof(int32_t), b->stream));
+    const cudaError_t le = rp::launchBatchedStep(A, plan, b->precision, b->stream);
+    b->launches += 1;
+    if (le != cudaSuccess) return fail(RP_ERR_CUDA, std::string("step launch failed: ") + cudaGetErrorString(le));
+    return RP_OK;
+}
+
 rp_status rp_batch_step_many(rp_batch* b, const rp_step_params* p, int32_t steps) {
     if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
     rp_status st = validateParams(p);

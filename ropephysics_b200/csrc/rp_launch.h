@@ -28,6 +28,10 @@ cudaError_t launchBatchedStep(const DArgs& a, const BatchedPlan& plan, int preci
 cudaError_t batchedReserveSmem(size_t bytes);
 cudaError_t batchedOccupancy(int threads, size_t smemBytes, int* blocksPerSm);
 
+// Address and size of this device's static scratch array (looked up on the
+// first call per device, with that device current).
+cudaError_t staticScratch(void** ptr, size_t* bytes);
+
 // One hold observation of every armed rod (the final sample of a run).
 cudaError_t launchObserve(const DArgs& a, int compensated, cudaStream_t stream);
 
