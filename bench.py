@@ -35,7 +35,8 @@ sys.path.insert(0, ROOT)
 
 # Floating-point operations per segment-substep of the plain step (add, sub,
 # mul, div, sqrt), counted exactly by the op-counting oracle build
-# (oracle/count_flops.py). Contacts add ~10 per (particle, primitive) slot.
+# (liboracle_count.so; tests/test_oracle.py pins these values). Contacts add
+# ~10 per (particle, primitive) slot.
 FLOPS_PER_SEG_SUBSTEP = {"grid": 890.5, "uneven": 880.5, "cantilever": 880.5}
 # Algorithmic HBM bytes per segment per step: state read once and written once
 # (x, v, force, kinematic velocity per particle; q, omega, torque per frame;
@@ -309,6 +310,9 @@ def run_ours(args):
     batch.set_stream(stream.cuda_stream)
     batch.set_graph(True)
     p = wl.params
+    # rods per CTA, threads per rod and steps per launch, timed on this batch
+    # (its state is restored afterwards)
+    tuning = batch.autotune(p, max_steps_per_launch=4) if not args.no_tune else batch.tuning
 
     # warm-up: first launches pay module load; the graph is captured here
     for _ in range(args.warmup):
@@ -401,7 +405,7 @@ def run_ours(args):
         "dtype": "f32",
         "data": "synthetic (seeded)",
         "config": {"workload": wl.name, "rods": len(wl.rods), "segments": int(wl.segments.sum()),
-                   "substeps": p.substeps, "dt": p.dt, "strategy": "batched",
+                   "substeps": p.substeps, "dt": p.dt, "strategy": "batched", "tuning": tuning,
                    "graph": True, "l2": "inputs larger than L2" if bytes_alg > 126e6 else "L2-resident state",
                    "parallelism": f"replicas{world_size}"},
         "e2e": {"value": e2e, "unit": "segment-substeps/s", "h2d_bytes_per_step": 16 * batch.total_particles,
@@ -456,7 +460,9 @@ def run_reference(args):
             "n_gpus": world_size, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded)", "impl": "reference",
-            "config": {"workload": wl.name, "rods": len(wl.rods), "substeps": wl.params.substeps},
+            "config": {"workload": wl.name, "rods": len(wl.rods), "segments": int(wl.segments.sum()),
+                       "substeps": wl.params.substeps, "dt": wl.params.dt,
+                       "parallelism": f"replicas{world_size}", "sample": "bounded CPU sample per step"},
             "cpu_baseline": {"value": value, "unit": "segment-substeps/s", "cores": threads,
                              "kind": kind, "sample": samples[-1]},
             "e2e": {"value": value, "unit": "segment-substeps/s", "h2d_bytes_per_step": 0,
@@ -474,6 +480,7 @@ def main():
     ap.add_argument("--rods", type=int, default=0)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-rods", type=int, default=64)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)

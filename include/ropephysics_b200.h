@@ -245,7 +245,8 @@ void rp_batch_destroy(rp_batch* batch);
 /* reference: Batch::step, gpu_solver.h:85, gpu_batch.cpp:457-473 */
 rp_status rp_batch_step(rp_batch* batch, const rp_step_params* params);
 /* `steps` steps; when graphs are enabled (rp_batch_set_graph) the sequence is
- * replayed from a captured CUDA graph. */
+ * replayed from a captured CUDA graph. The batched strategy runs up to its
+ * tuned steps-per-launch whole steps in one launch (same results). */
 rp_status rp_batch_step_many(rp_batch* batch, const rp_step_params* params, int32_t steps);
 /* No reference counterpart. One step of an RP_STRATEGY_BATCHED batch, the
  * same kernel and the same results as rp_batch_step, but the step's scratch
@@ -270,6 +271,18 @@ rp_status rp_batch_set_precision(rp_batch* batch, int32_t flags);
 /* Capture rp_batch_step_many sequences into CUDA graphs (1) or launch
  * directly (0, default). */
 rp_status rp_batch_set_graph(rp_batch* batch, int32_t enabled);
+/* Launch shape of RP_STRATEGY_BATCHED: CTA size (128 or 256 threads; rods per
+ * CTA = CTA size / team size), pairs per thread (a rod of n segments gets a
+ * team of about n / (2 x pairs) threads, whole warps, 32..256) and whole steps
+ * per launch in rp_batch_step_many. None of them changes results.
+ * rp_batch_autotune times the candidate shapes on this batch with its current
+ * state (restored afterwards) and keeps the fastest; steps per launch is
+ * tried up to max_steps_per_launch (at most 8). */
+rp_status rp_batch_autotune(rp_batch* batch, const rp_step_params* params, int32_t max_steps_per_launch);
+rp_status rp_batch_get_tuning(const rp_batch* batch, int32_t* cta_threads, int32_t* pairs_per_thread,
+                              int32_t* steps_per_launch);
+rp_status rp_batch_set_tuning(rp_batch* batch, int32_t cta_threads, int32_t pairs_per_thread,
+                              int32_t steps_per_launch);
 
 /* reference: Batch::download(rodIndex, Rod&), gpu_solver.h:90. Writes x, v,
  * q and omega of rod `rod` into `out`'s arrays (same topology). */

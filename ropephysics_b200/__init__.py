@@ -427,6 +427,22 @@ class Batch:
     def set_graph(self, enabled: bool):
         _check(lib().rp_batch_set_graph(self._h, int(enabled)))
 
+    def autotune(self, params: StepParams, max_steps_per_launch: int = 4) -> dict:
+        """Time the batched launch shapes on this batch (state restored after)
+        and keep the fastest; returns the chosen tuning."""
+        p = params.to_c()
+        _check(lib().rp_batch_autotune(self._h, C.byref(p), max_steps_per_launch))
+        return self.tuning
+
+    @property
+    def tuning(self) -> dict:
+        a, b, c = C.c_int32(), C.c_int32(), C.c_int32()
+        _check(lib().rp_batch_get_tuning(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return {"cta_threads": a.value, "pairs_per_thread": b.value, "steps_per_launch": c.value}
+
+    def set_tuning(self, cta_threads: int = 256, pairs_per_thread: int = 1, steps_per_launch: int = 1):
+        _check(lib().rp_batch_set_tuning(self._h, cta_threads, pairs_per_thread, steps_per_launch))
+
     # ---- state transfer ----
     def download(self, rod_index: int, rod: Rod):
         _check(lib().rp_batch_download(self._h, rod_index, C.byref(rod.desc)))

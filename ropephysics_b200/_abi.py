@@ -108,6 +108,9 @@ SIGNATURES = {
     "rp_batch_step": (i32, [vp, P(StepParams)]),
     "rp_batch_step_many": (i32, [vp, P(StepParams), i32]),
     "rp_batch_step_static_scratch": (i32, [vp, P(StepParams)]),
+    "rp_batch_autotune": (i32, [vp, P(StepParams), i32]),
+    "rp_batch_get_tuning": (i32, [vp, P(C.c_int32), P(C.c_int32), P(C.c_int32)]),
+    "rp_batch_set_tuning": (i32, [vp, i32, i32, i32]),
     "rp_batch_synchronize": (i32, [vp]),
     "rp_batch_set_stream": (i32, [vp, vp]),
     "rp_batch_set_precision": (i32, [vp, i32]),

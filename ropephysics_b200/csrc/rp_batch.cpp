@@ -50,10 +50,11 @@ using rpx::fail;
 
 namespace {
 
-// Autotuned launch choices for the batched form (see rp_tune.cpp).
+// Launch choices for the batched form, picked by rp_batch_autotune.
 struct Tune {
-    int ctaThreads = 256;
-    int pairsPerThread = 1;  // team threads ~ ceil(nSt / 2 / pairsPerThread), rounded to 32
+    int ctaThreads = 256;     // threads per CTA (rods per CTA = ctaThreads / team)
+    int pairsPerThread = 1;   // team threads ~ ceil(nSt / 2 / pairsPerThread), rounded to 32
+    int stepsPerLaunch = 1;   // whole steps (x substeps) per launch in rp_batch_step_many
 };
 
 }  // namespace
@@ -98,6 +99,8 @@ struct rp_batch {
     bool useGraph = false;
     cudaGraphExec_t graphExec = nullptr;
     int graphSteps = 0;
+    int graphStepsPerLaunch = 0;
+    long long graphLaunches = 0;  // kernel launches in the captured graph
     rp_step_params graphParams{};
     int graphPrecision = -1;
 
@@ -528,9 +531,12 @@ rp_status validateParams(const rp_step_params* p) {
     return RP_OK;
 }
 
-rp_status launchStep(rp_batch* b, const rp_step_params* p) {
+// One launch of `steps` whole steps (more than one only for the batched
+// strategy, whose kernel keeps each rod on chip across them).
+rp_status launchStep(rp_batch* b, const rp_step_params* p, int steps = 1) {
     DArgs A = b->a;
     fillStepArgs(b, p, A);
+    A.stepsPerLaunch = steps;
     cudaError_t e;
     if (b->strategy == RP_STRATEGY_BATCHED) {
         rp::BatchedPlan plan;
@@ -686,12 +692,21 @@ rp_status rp_batch_step_many(rp_batch* b, const rp_step_params* p, int32_t steps
     if (st != RP_OK) return st;
     if (steps < 0) return fail(RP_ERR_INVALID, "steps < 0");
     if (steps == 0) return RP_OK;
-    if (!b->useGraph) {
-        for (int s = 0; s < steps; ++s)
-            if ((st = launchStep(b, p)) != RP_OK) return st;
+    // the batched kernel runs up to tune.stepsPerLaunch steps per launch;
+    // the result is the same as one launch per step
+    const int perLaunch = b->strategy == RP_STRATEGY_BATCHED ? std::max(1, b->tune.stepsPerLaunch) : 1;
+    auto launchAll = [&]() -> rp_status {
+        for (int done = 0; done < steps;) {
+            const int k = std::min(perLaunch, steps - done);
+            const rp_status s2 = launchStep(b, p, k);
+            if (s2 != RP_OK) return s2;
+            done += k;
+        }
         return RP_OK;
-    }
+    };
+    if (!b->useGraph) return launchAll();
     const bool same = b->graphExec && b->graphSteps == steps && b->graphPrecision == b->precision &&
+                      b->graphStepsPerLaunch == perLaunch &&
                       std::memcmp(&b->graphParams, p, sizeof(rp_step_params)) == 0;
     if (!same) {
         if (b->graphExec) {
@@ -701,25 +716,25 @@ rp_status rp_batch_step_many(rp_batch* b, const rp_step_params* p, int32_t steps
         cudaGraph_t graph = nullptr;
         RP_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
         const long long before = b->launches;
-        for (int s = 0; s < steps; ++s) {
-            st = launchStep(b, p);
-            if (st != RP_OK) {
-                cudaStreamEndCapture(b->stream, &graph);
-                if (graph) cudaGraphDestroy(graph);
-                return st;
-            }
+        st = launchAll();
+        if (st != RP_OK) {
+            cudaStreamEndCapture(b->stream, &graph);
+            if (graph) cudaGraphDestroy(graph);
+            return st;
         }
+        b->graphLaunches = b->launches - before;
         b->launches = before;
         RP_CUDA(cudaStreamEndCapture(b->stream, &graph));
         const cudaError_t e = cudaGraphInstantiate(&b->graphExec, graph, 0);
         cudaGraphDestroy(graph);
         if (e != cudaSuccess) return fail(RP_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
         b->graphSteps = steps;
+        b->graphStepsPerLaunch = perLaunch;
         b->graphParams = *p;
         b->graphPrecision = b->precision;
     }
     RP_CUDA(cudaGraphLaunch(b->graphExec, b->stream));
-    b->launches += int64_t(steps);
+    b->launches += b->graphLaunches;
     return RP_OK;
 }
 
@@ -765,6 +780,182 @@ rp_status rp_batch_set_precision(rp_batch* b, int32_t flags) {
         }
     }
     b->precision = flags;
+    return RP_OK;
+}
+
+rp_status rp_batch_get_tuning(const rp_batch* b, int32_t* cta_threads, int32_t* pairs_per_thread,
+                              int32_t* steps_per_launch) {
+    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
+    if (cta_threads) *cta_threads = b->tune.ctaThreads;
+    if (pairs_per_thread) *pairs_per_thread = b->tune.pairsPerThread;
+    if (steps_per_launch) *steps_per_launch = b->tune.stepsPerLaunch;
+    return RP_OK;
+}
+
+rp_status rp_batch_set_tuning(rp_batch* b, int32_t cta_threads, int32_t pairs_per_thread,
+                              int32_t steps_per_launch) {
+    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
+    if (b->strategy != RP_STRATEGY_BATCHED) return fail(RP_ERR_INVALID, "tuning applies to RP_STRATEGY_BATCHED");
+    if (cta_threads != 128 && cta_threads != 256)
+        return fail(RP_ERR_INVALID, "cta_threads must be 128 or 256");
+    if (pairs_per_thread < 1 || pairs_per_thread > 8)
+        return fail(RP_ERR_INVALID, "pairs_per_thread must be in 1..8");
+    if (steps_per_launch < 1 || steps_per_launch > 64)
+        return fail(RP_ERR_INVALID, "steps_per_launch must be in 1..64");
+    rp_status st = syncBatch(b);
+    if (st != RP_OK) return st;
+    const Tune old = b->tune;
+    b->tune.ctaThreads = cta_threads;
+    b->tune.pairsPerThread = pairs_per_thread;
+    b->tune.stepsPerLaunch = steps_per_launch;
+    if (old.ctaThreads != cta_threads || old.pairsPerThread != pairs_per_thread) {
+        st = buildBatchedPlan(b);
+        if (st != RP_OK) {
+            b->tune = old;
+            const rp_status st2 = buildBatchedPlan(b);
+            return st2 != RP_OK ? st2 : st;
+        }
+    }
+    if (b->graphExec) {
+        cudaGraphExecDestroy(b->graphExec);
+        b->graphExec = nullptr;
+    }
+    return RP_OK;
+}
+
+namespace {
+
+// Device copies of everything a step changes, so tuning trials leave the
+// batch as they found it.
+struct StateSnapshot {
+    std::vector<std::pair<void*, size_t>> regions;
+    std::vector<void*> copies;
+    ~StateSnapshot() {
+        for (void* c : copies) cudaFree(c);
+    }
+    rp_status take(rp_batch* b) {
+        const DArgs& A = b->a;
+        const size_t P = size_t(b->totalP), S = size_t(b->totalS), R = size_t(b->numRods);
+        auto add = [&](const void* p, size_t bytes) {
+            if (p && bytes) regions.emplace_back(const_cast<void*>(p), bytes);
+        };
+        add(A.x, P * 16);
+        add(A.v, P * 16);
+        add(A.xComp, P * 16);
+        add(A.kinVel, P * 16);
+        add(A.q, S * 16);
+        add(A.omega, S * 16);
+        add(A.contactState, size_t(b->totalSlots));
+        add(A.selfCount, R * 4);
+        add(A.selfOverflow, R * 4);
+        add(A.selfPairs, size_t(b->totalPool) * 4);
+        add(A.errors, R * 4);
+        add(A.rodTime, R * 8);
+        add(A.hold, R * sizeof(rp::DHold));
+        for (auto& rg : regions) {
+            void* c = nullptr;
+            if (cudaMalloc(&c, rg.second) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(RP_ERR_OUT_OF_MEMORY, "autotune: no room for the state snapshot");
+            }
+            copies.push_back(c);
+            RP_CUDA(cudaMemcpyAsync(c, rg.first, rg.second, cudaMemcpyDeviceToDevice, b->stream));
+        }
+        return RP_OK;
+    }
+    rp_status restore(rp_batch* b) {
+        for (size_t i = 0; i < regions.size(); ++i)
+            RP_CUDA(cudaMemcpyAsync(regions[i].first, copies[i], regions[i].second, cudaMemcpyDeviceToDevice,
+                                    b->stream));
+        return RP_OK;
+    }
+};
+
+// Device milliseconds per step of `launches` launches of `k` steps each.
+rp_status timeSteps(rp_batch* b, const rp_step_params* p, int k, int launches, float* msPerStep) {
+    cudaEvent_t e0, e1;
+    RP_CUDA(cudaEventCreate(&e0));
+    RP_CUDA(cudaEventCreate(&e1));
+    rp_status st = RP_OK;
+    cudaEventRecord(e0, b->stream);
+    for (int i = 0; i < launches && st == RP_OK; ++i) st = launchStep(b, p, k);
+    cudaEventRecord(e1, b->stream);
+    const cudaError_t e = cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    if (st == RP_OK && e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != RP_OK) return st;
+    if (e != cudaSuccess) return fail(RP_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(e));
+    *msPerStep = ms / float(k * launches);
+    return RP_OK;
+}
+
+}  // namespace
+
+rp_status rp_batch_autotune(rp_batch* b, const rp_step_params* p, int32_t max_steps_per_launch) {
+    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
+    rp_status st = validateParams(p);
+    if (st != RP_OK) return st;
+    if (b->strategy != RP_STRATEGY_BATCHED) return fail(RP_ERR_INVALID, "tuning applies to RP_STRATEGY_BATCHED");
+    if (max_steps_per_launch < 1) return fail(RP_ERR_INVALID, "max_steps_per_launch must be >= 1");
+    if ((st = syncBatch(b)) != RP_OK) return st;
+    StateSnapshot snap;
+    if ((st = snap.take(b)) != RP_OK) return st;
+    const long long launches0 = b->launches;
+    const Tune start = b->tune;
+    Tune best = start;
+    float bestMs = 3.0e38f;
+    // rods per CTA and threads per rod: every (CTA size, team size) pair that
+    // plans, one warm launch and two timed launches from the same state
+    for (int cta : {128, 256}) {
+        for (int ppt : {1, 2}) {
+            b->tune.ctaThreads = cta;
+            b->tune.pairsPerThread = ppt;
+            b->tune.stepsPerLaunch = 1;
+            if (buildBatchedPlan(b) != RP_OK) continue;
+            float ms = 0.0f;
+            if ((st = snap.restore(b)) != RP_OK) break;
+            if ((st = launchStep(b, p, 1)) != RP_OK) break;
+            if ((st = snap.restore(b)) != RP_OK) break;
+            if ((st = timeSteps(b, p, 1, 2, &ms)) != RP_OK) break;
+            if (ms < bestMs) {
+                bestMs = ms;
+                best = b->tune;
+            }
+        }
+        if (st != RP_OK) break;
+    }
+    // whole steps per launch, on the chosen shape; a longer launch must win
+    // by 2 % to be kept
+    if (st == RP_OK && bestMs < 3.0e38f) {
+        b->tune = best;
+        st = buildBatchedPlan(b);
+        for (int k = 2; st == RP_OK && k <= max_steps_per_launch && k <= 8; k *= 2) {
+            float ms = 0.0f;
+            if ((st = snap.restore(b)) != RP_OK) break;
+            if ((st = timeSteps(b, p, k, 1, &ms)) != RP_OK) break;
+            if (ms < bestMs * 0.98f) {
+                bestMs = ms;
+                best.stepsPerLaunch = k;
+            }
+        }
+    }
+    const rp_status trial = st;
+    b->tune = trial == RP_OK ? best : start;
+    st = buildBatchedPlan(b);
+    const rp_status back = snap.restore(b);
+    const rp_status sync = syncBatch(b);
+    b->launches = launches0;
+    if (b->graphExec) {
+        cudaGraphExecDestroy(b->graphExec);
+        b->graphExec = nullptr;
+    }
+    if (trial != RP_OK) return trial;
+    if (st != RP_OK) return st;
+    if (back != RP_OK) return back;
+    if (sync != RP_OK) return sync;
+    if (bestMs >= 3.0e38f) return fail(RP_ERR_SHARED_MEMORY, "autotune: no launch shape fits");
     return RP_OK;
 }
 

@@ -10,18 +10,28 @@
 //
 // Inside a team the colour sweeps are separated by __syncwarp (one-warp teams)
 // or a named barrier (bar.sync id, team) instead of a CTA-wide barrier, and
-// the serial parts of the reference's self-collision broad phase run in
-// parallel while keeping its exact order:
-//   * centres, cell size (max is exact in any order), bucket counts (integer);
-//   * exclusive scans of bucket counts and per-segment contact counts across
-//     the team (integer, deterministic);
-//   * the stable counting-sort placement by one warp walking the segments in
-//     order 32 at a time, ranking equal buckets with __match_any_sync.
-// The pool is then exactly the reference's list (segments ascending, 3x3x3
-// cells z/y/x, bucket order), and its projection stays sequential in that
-// order. Every per-element operation is the shared code in
-// rp_step_common.cuh, so results are bit-identical to the plain kernel.
+// the reference's self-collision pipeline (hash build, count pass, prefix sum,
+// fill pass, sequential projection) is reorganised without changing its
+// result:
+//   * counting: the reference counts, for segment j, every later segment k
+//     (k - j >= gap) in the hash buckets of the 27 cells around j whose
+//     segments touch (separation < 0). A touching k sits in one bucket,
+//     hash(cell(k)), so it is counted once per cell of the 27 whose hash is
+//     that bucket. Touching pairs are found here by a broad phase over chain
+//     blocks of 8 consecutive segments (box-distance culling with a bound no
+//     tighter than the per-pair sphere test, then the per-pair test and the
+//     shared narrow phase), each weighted by that multiplicity: the same
+//     counts, without building the hash when nothing touches;
+//   * when something touches, the hash is built (stable counting sort: team
+//     scans and one warp placing segments in order with __match_any_sync) and
+//     the reference's fill pass writes the pool in its exact order;
+//   * the pool is projected level by level (contacts of a level share no
+//     particle), which reproduces the sequential order's arithmetic.
+// Every per-element operation is the shared code in rp_step_common.cuh, so
+// results are bit-identical to the plain kernel.
 #include <cuda_runtime.h>
+
+#include <mutex>
 
 #include "rp_launch.h"
 #include "rp_layout.h"
@@ -37,6 +47,23 @@ __device__ __forceinline__ void teamSync(int team, int teamIdx) {
     } else {
         asm volatile("bar.sync %0, %1;" ::"r"(teamIdx + 1), "r"(team) : "memory");
     }
+}
+
+// Order-preserving map of a float to an unsigned (negative values
+// reversed), so a warp's float min or max is one integer reduction
+// (redux.sync). Min and max are exact, so the result is one of the inputs.
+__device__ __forceinline__ unsigned orderedKey(float f) {
+    const unsigned u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float fromOrderedKey(unsigned k) {
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+__device__ __forceinline__ float warpMax(float f) {
+    return fromOrderedKey(__reduce_max_sync(0xffffffffu, orderedKey(f)));
+}
+__device__ __forceinline__ float warpMin(float f) {
+    return fromOrderedKey(__reduce_min_sync(0xffffffffu, orderedKey(f)));
 }
 
 __device__ __forceinline__ float4 driveVelocityB(const DDrive& d, double t) {
@@ -79,6 +106,79 @@ __device__ int teamExclusiveScan(int32_t* a, int m, int lane, int team, int team
     return total;
 }
 
+// Multiplicity of a touching pair in the reference's count: the number of
+// the 27 cells around cell(j) whose hash is k's bucket hash(cell(k)).
+__device__ __forceinline__ int bucketMultiplicity(float4 cj, float4 ck, float cell, int table) {
+    const int cx = cellCoord(cj.x, cell), cy = cellCoord(cj.y, cell), cz = cellCoord(cj.z, cell);
+    const unsigned hk = hashCell(cellCoord(ck.x, cell), cellCoord(ck.y, cell), cellCoord(ck.z, cell), table);
+    int m = 0;
+    for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx) m += hashCell(cx + dx, cy + dy, cz + dz, table) == hk ? 1 : 0;
+    return m;
+}
+
+// segCount[j] (zeroed by the caller) += the reference's count of segment j.
+// Warp w of the team takes chain blocks J = w, w + warps, ...; its lanes test
+// 32 blocks K >= J at a time against J by box distance, and for each block
+// that can hold a pair within the sphere bound the warp runs the 64 segment
+// pairs (j in J, k in K), two per lane: the per-pair sphere test of
+// querySelfSegment, then the shared narrow phase. The box test skips only
+// when box distance^2 > 1.0001 x bound^2 with every per-pair quantity bounded
+// by its block maximum (float max, add and multiply are monotone), so every
+// pair the sphere test keeps is reached.
+__device__ void countSelfByBlocks(const RodView& V, const SelfScratch& S, int nSt, int gap, int table,
+                                  int lane, int team, int32_t* touching) {
+    if (nSt <= gap) return;
+    const int wl = lane & 31, warp = lane >> 5, warps = team >> 5;
+    const int nBlk = (nSt + 7) >> 3;
+    const float twoR = 2.0f * V.radius;
+    const float cell = *S.cellSize;
+    for (int J = warp; J < nBlk; J += warps) {
+        const float4 jlo = S.blocks[2 * J], jhi = S.blocks[2 * J + 1];
+        const int jmin = 8 * J;
+        // this lane's segment of J for the pair tests
+        const int j = jmin + (wl & 7);
+        const float4 cj = j < nSt ? S.centres[j] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        const float scaleSlack = 1e-6f * (1.0f + fabsf(cj.x) + fabsf(cj.y) + fabsf(cj.z));
+        for (int K0 = J; K0 < nBlk; K0 += 32) {
+            const int K = K0 + wl;
+            bool hit = false;
+            if (K < nBlk && min(8 * K + 7, nSt - 1) - jmin >= gap) {
+                const float4 klo = S.blocks[2 * K], khi = S.blocks[2 * K + 1];
+                const float gx = fmaxf(0.0f, fmaxf(klo.x - jhi.x, jlo.x - khi.x));
+                const float gy = fmaxf(0.0f, fmaxf(klo.y - jhi.y, jlo.y - khi.y));
+                const float gz = fmaxf(0.0f, fmaxf(klo.z - jhi.z, jlo.z - khi.z));
+                const float lim = (jlo.w + klo.w + twoR) * 1.001f + 1e-6f * jhi.w;
+                hit = !(gx * gx + gy * gy + gz * gz > lim * lim * 1.0001f);
+            }
+            unsigned m = __ballot_sync(0xffffffffu, hit);
+            while (m) {
+                const int Kh = K0 + __ffs(m) - 1;
+                m &= m - 1u;
+#pragma unroll
+                for (int h2 = 0; h2 < 2; ++h2) {
+                    const int k = 8 * Kh + (wl >> 3) + 4 * h2;
+                    if (j >= nSt || k >= nSt || k - j < gap) continue;
+                    const float4 ck = S.centres[k];
+                    const float ddx = ck.x - cj.x, ddy = ck.y - cj.y, ddz = ck.z - cj.z;
+                    const float bound = cj.w + ck.w + twoR;
+                    const float plim = bound * 1.001f + scaleSlack;
+                    if (ddx * ddx + ddy * ddy + ddz * ddz > plim * plim) continue;
+                    const SegPair P = segmentPairNarrow(v3(V.x[V.sP0[j]]), v3(V.x[V.sP1[j]]),
+                                                        v3(V.x[V.sP0[k]]), v3(V.x[V.sP1[k]]), twoR);
+                    if (P.separation >= 0.0f) continue;
+                    const int mult = bucketMultiplicity(cj, ck, cell, table);
+                    if (mult) {
+                        atomicAdd(&S.segCount[j], mult);
+                        *touching = 1;
+                    }
+                }
+            }
+        }
+    }
+}
+
 template <bool COMP, bool FP64>
 __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int team, int teamIdx) {
     const DRod R = A.rods[r];
@@ -111,11 +211,11 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
     V.x = reinterpret_cast<float4*>(base + L.x);
     V.xPrev = reinterpret_cast<float4*>(base + L.xPrev);
     V.xComp = COMP ? reinterpret_cast<float4*>(base + L.xComp) : A.xComp + R.pOff;
-    // lean layout: velocities, angular velocities and loads stay in global memory
-    V.v = A.v + R.pOff;
+    // lean layout: loads and kinematic velocities stay in global memory
+    V.v = reinterpret_cast<float4*>(base + L.v);
     V.force = A.force + R.pOff;
     V.kin = A.kinVel + R.pOff;
-    V.omega = A.omega + R.sOff;
+    V.omega = reinterpret_cast<float4*>(base + L.omega);
     V.torque = A.torque + R.sOff;
     V.lamS = reinterpret_cast<float4*>(base + L.lamS);
     V.lamB = reinterpret_cast<float4*>(base + L.lamB);
@@ -133,9 +233,11 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
     S.cellSize = reinterpret_cast<float*>(misc);
     S.live = misc + 1;
     S.overflow = misc + 2;
+    S.blocks = reinterpret_cast<float4*>(base + L.blocks);
     int32_t* partial = misc + 4;  // one per warp of the team (up to 8)
     int32_t* numLevels = misc + 3;
     unsigned long long* primMask = reinterpret_cast<unsigned long long*>(misc + 12);
+    int32_t* touching = misc + 14;  // some segment pair touches this substep
     float* red = reinterpret_cast<float*>(misc + 16);  // 8 floats per warp
     int32_t* lvlOrder = reinterpret_cast<int32_t*>(base + L.levels);
     int32_t* lvlStart = lvlOrder + (R.selfCapacity + 1);
@@ -145,29 +247,33 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
         *primMask = ~0ull;
     }
 
+    // simulated time of this rod, advanced per step exactly as the
+    // one-step-per-launch path advances rodTime[r]
+    double tRod = A.rodTime[r];
     int driveP = -1;
-    float4 driveV = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    DDrive drive{};
     if (A.drives) {
-        const DDrive d = A.drives[r];
-        if (d.particle >= 0 && d.particle < nP) {
-            driveP = d.particle;
-            driveV = driveVelocityB(d, A.rodTime[r]);
-        }
+        drive = A.drives[r];
+        if (drive.particle >= 0 && drive.particle < nP) driveP = drive.particle;
     }
 
     // ---- stage in (coalesced float4 rows) ----
     {
         const float4* gx = A.x + R.pOff;
+        const float4* gv = A.v + R.pOff;
         const float4* gc = A.xComp + R.pOff;
         for (int i = lane; i < nP; i += team) {
             V.x[i] = gx[i];
+            V.v[i] = gv[i];
             if (COMP) V.xComp[i] = gc[i];
         }
         const float4* gq = A.q + R.sOff;
-        for (int j = lane; j < nS; j += team) V.q[j] = gq[j];
-        if (driveP >= 0 && lane == 0) V.kin[driveP] = driveV;
+        const float4* gw = A.omega + R.sOff;
+        for (int j = lane; j < nS; j += team) {
+            V.q[j] = gq[j];
+            V.omega[j] = gw[j];
+        }
     }
-    teamSync(team, teamIdx);
 
     const V3 g{A.gx, A.gy, A.gz};
     const float h = A.h, invH2 = A.invH2;
@@ -179,192 +285,273 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
     const bool self = R.selfCollision != 0;
     const int table = R.hashTableSize;
 
-    for (int sub = 0; sub < A.substeps; ++sub) {
-        for (int k = lane; k < nSt; k += team) V.lamS[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        for (int k = lane; k < nB; k += team) V.lamB[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        const bool regenerate = sub % interval == 0;
-        if (regenerate && (V.numPrims > 0 || self)) {
-            // One pass for both contact kinds: segment centres and half
-            // lengths, the longest segment (self-collision cell size), and the
-            // rod's bounding box (primitive culling).
-            float mx = 0.0f;
-            float lx = 3.0e38f, ly = 3.0e38f, lz = 3.0e38f;
-            float hx = -3.0e38f, hy = -3.0e38f, hz = -3.0e38f;
-            if (self) {
-                for (int j = lane; j < nSt; j += team) {
-                    const V3 a = v3(V.x[V.sP0[j]]), b = v3(V.x[V.sP1[j]]);
-                    const float len = norm(b - a);
-                    const V3 c = (a + b) * 0.5f;
-                    S.centres[j] = make_float4(c.x, c.y, c.z, 0.5f * len);
-                    mx = fmaxf(mx, len);
-                }
-                for (int t = lane; t <= table; t += team) S.cellStart[t] = 0;
-            }
-            if (V.numPrims > 0) {
-                for (int i = lane; i < nP; i += team) {
-                    const float4 p = V.x[i];
-                    lx = fminf(lx, p.x); ly = fminf(ly, p.y); lz = fminf(lz, p.z);
-                    hx = fmaxf(hx, p.x); hy = fmaxf(hy, p.y); hz = fmaxf(hz, p.z);
-                }
-            }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-                lx = fminf(lx, __shfl_xor_sync(0xffffffffu, lx, o));
-                ly = fminf(ly, __shfl_xor_sync(0xffffffffu, ly, o));
-                lz = fminf(lz, __shfl_xor_sync(0xffffffffu, lz, o));
-                hx = fmaxf(hx, __shfl_xor_sync(0xffffffffu, hx, o));
-                hy = fmaxf(hy, __shfl_xor_sync(0xffffffffu, hy, o));
-                hz = fmaxf(hz, __shfl_xor_sync(0xffffffffu, hz, o));
-            }
-            if ((lane & 31) == 0) {
-                float* row = red + 8 * (lane >> 5);
-                row[0] = mx; row[1] = lx; row[2] = ly; row[3] = lz;
-                row[4] = hx; row[5] = hy; row[6] = hz;
-            }
-            teamSync(team, teamIdx);
-            for (int w = 0; w < (team >> 5); ++w) {
-                const float* row = red + 8 * w;
-                mx = fmaxf(mx, row[0]);
-                lx = fminf(lx, row[1]); ly = fminf(ly, row[2]); lz = fminf(lz, row[3]);
-                hx = fmaxf(hx, row[4]); hy = fmaxf(hy, row[5]); hz = fmaxf(hz, row[6]);
-            }
-            if (V.numPrims > 0 && lane == 0)
-                *primMask = primitivesNearBox(V, V3{lx, ly, lz}, V3{hx, hy, hz});
-            if (self && lane == 0) {
-                if (sub == 0) *S.overflow = 0;
-                *S.cellSize = mx + 2.0f * V.radius;
-            }
-            teamSync(team, teamIdx);  // mask and cell size visible; rows reusable
-        }
-        if (V.numPrims > 0) {
-            const unsigned long long mask = *primMask;
-            for (int i = lane; i < nP; i += team) generateSlotsMasked(V, i, regenerate, mask);
-        }
-        if (self) {
-            if (regenerate) {
-                const float cell = *S.cellSize;
-                for (int j = lane; j < nSt; j += team) {
-                    const float4 c = S.centres[j];
-                    const int h0 = int(hashCell(cellCoord(c.x, cell), cellCoord(c.y, cell),
-                                                cellCoord(c.z, cell), table));
-                    S.cellOf[j] = h0;
-                    atomicAdd(&S.cellStart[h0], 1);
-                }
-                teamSync(team, teamIdx);
-                // counts -> starts: cellStart[t] = first slot of bucket t,
-                // cellStart[table] = segment count (the reference's offsets)
-                teamExclusiveScan(S.cellStart, table + 1, lane, team, teamIdx, partial);
-                for (int t = lane; t < table; t += team) cursor[t] = S.cellStart[t];
-                teamSync(team, teamIdx);
-                // stable placement, one warp walking segments in order
-                if (lane < 32) {
-                    for (int j0 = 0; j0 < nSt; j0 += 32) {
-                        const int j = j0 + lane;
-                        const bool valid = j < nSt;
-                        const int c = valid ? S.cellOf[j] : -1 - lane;
-                        const unsigned peers = __match_any_sync(0xffffffffu, c);
-                        const int rank = __popc(peers & ((1u << lane) - 1u));
-                        const int start = valid ? cursor[c] : 0;
-                        __syncwarp();
-                        if (valid) {
-                            S.sorted[start + rank] = j;
-                            if (rank == 0) cursor[c] = start + __popc(peers);
-                        }
-                        __syncwarp();
+    const int stepsHere = A.stepsPerLaunch > 0 ? A.stepsPerLaunch : 1;
+    for (int step = 0; step < stepsHere; ++step) {
+        if (driveP >= 0 && lane == 0) V.kin[driveP] = driveVelocityB(drive, tRod);
+        teamSync(team, teamIdx);
+        for (int sub = 0; sub < A.substeps; ++sub) {
+            for (int k = lane; k < nSt; k += team) V.lamS[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            for (int k = lane; k < nB; k += team) V.lamB[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            const bool regenerate = sub % interval == 0;
+            unsigned long long maskNow = *primMask;  // this substep's primitive cull
+            float cellNow = 0.0f;                    // this substep's self-collision cell
+            if (regenerate && (V.numPrims > 0 || self)) {
+                // One pass for both contact kinds: segment centres and half
+                // lengths, the longest segment (self-collision cell size), and the
+                // rod's bounding box (primitive culling).
+                float mx = 0.0f;
+                float lx = 3.0e38f, ly = 3.0e38f, lz = 3.0e38f;
+                float hx = -3.0e38f, hy = -3.0e38f, hz = -3.0e38f;
+                if (self) {
+                    for (int j = lane; j < nSt; j += team) {
+                        const int p0 = T.chain ? j : V.sP0[j], p1 = T.chain ? j + 1 : V.sP1[j];
+                        const V3 a = v3(V.x[p0]), b = v3(V.x[p1]);
+                        const float len = norm(b - a);
+                        const V3 c = (a + b) * 0.5f;
+                        S.centres[j] = make_float4(c.x, c.y, c.z, 0.5f * len);
+                        mx = fmaxf(mx, len);
                     }
                 }
-                teamSync(team, teamIdx);
-                for (int j = lane; j < nSt; j += team)
-                    querySelfSegment<true>(V, S, j, nSt, R.selfGap, table, R.selfCapacity,
-                                           R.selfFriction, false);
-                teamSync(team, teamIdx);
-                for (int j = lane; j < nSt; j += team) S.segStart[j] = S.segCount[j];
-                teamSync(team, teamIdx);
-                const int total = teamExclusiveScan(S.segStart, nSt, lane, team, teamIdx, partial);
-                const int live = total < R.selfCapacity ? total : R.selfCapacity;
-                if (lane == 0) {
-                    *S.live = live;
-                    if (total > R.selfCapacity) *S.overflow += total - R.selfCapacity;
+                if (V.numPrims > 0) {
+                    for (int i = lane; i < nP; i += team) {
+                        const float4 p = V.x[i];
+                        lx = fminf(lx, p.x); ly = fminf(ly, p.y); lz = fminf(lz, p.z);
+                        hx = fmaxf(hx, p.x); hy = fmaxf(hy, p.y); hz = fmaxf(hz, p.z);
+                    }
                 }
-                if (live > 0) {
-                    for (int j = lane; j < nSt; j += team)
-                        querySelfSegment<true>(V, S, j, nSt, R.selfGap, table, R.selfCapacity,
-                                               R.selfFriction, true);
-                    // every thread is done reading the hash (sorted) before
-                    // cellOf and sorted (2 nSt >= nP ints) are reused below
-                    teamSync(team, teamIdx);
-                    for (int i = lane; i < nP; i += team) S.cellOf[i] = 0;
-                    teamSync(team, teamIdx);
-                    if (lane == 0) {
-                        int kept = live;
-                        *numLevels = buildProjectionLevels(S.pool, live, nP, S.cellOf, lvlOf, lvlOrder,
-                                                           lvlStart, &kept);
-                        if (kept != live) {
-                            // a pool entry indexed outside the rod: keep the valid
-                            // prefix and report it, never touch memory with it
-                            *S.live = kept;
-                            if (A.errors) atomicOr(A.errors + r, 1);
+                mx = warpMax(mx);
+                lx = warpMin(lx);
+                ly = warpMin(ly);
+                lz = warpMin(lz);
+                hx = warpMax(hx);
+                hy = warpMax(hy);
+                hz = warpMax(hz);
+                if ((lane & 31) == 0) {
+                    float* row = red + 8 * (lane >> 5);
+                    row[0] = mx; row[1] = lx; row[2] = ly; row[3] = lz;
+                    row[4] = hx; row[5] = hy; row[6] = hz;
+                }
+                teamSync(team, teamIdx);  // centres and per-warp rows visible
+                // every lane reduces the rows in the same order (max and min
+                // are exact), so every lane holds the same mask and cell size;
+                // lane 0 also publishes them for the later phases
+                for (int w = 0; w < (team >> 5); ++w) {
+                    const float* row = red + 8 * w;
+                    mx = fmaxf(mx, row[0]);
+                    lx = fminf(lx, row[1]); ly = fminf(ly, row[2]); lz = fminf(lz, row[3]);
+                    hx = fmaxf(hx, row[4]); hy = fmaxf(hy, row[5]); hz = fmaxf(hz, row[6]);
+                }
+                if (V.numPrims > 0) {
+                    maskNow = primitivesNearBox(V, V3{lx, ly, lz}, V3{hx, hy, hz});
+                    if (lane == 0) *primMask = maskNow;
+                }
+                cellNow = mx + 2.0f * V.radius;
+                if (self && lane == 0) {
+                    if (sub == 0) *S.overflow = 0;
+                    *S.cellSize = cellNow;
+                    *touching = 0;
+                }
+            }
+            if (V.numPrims > 0) {
+                for (int i = lane; i < nP; i += team) generateSlotsMasked(V, i, regenerate, maskNow);
+            }
+            if (self) {
+                if (regenerate) {
+                    const float cell = cellNow;
+                    // ---- count: contacts per segment, by chain blocks ----
+                    const int nBlk = (nSt + 7) >> 3;
+                    for (int b = lane; b < nBlk; b += team) {
+                        float4 lo = make_float4(3.0e38f, 3.0e38f, 3.0e38f, 0.0f);
+                        float4 hi = make_float4(-3.0e38f, -3.0e38f, -3.0e38f, 0.0f);
+                        const int j1 = min(8 * b + 8, nSt);
+                        for (int j = 8 * b; j < j1; ++j) {
+                            const float4 c = S.centres[j];
+                            lo.x = fminf(lo.x, c.x); lo.y = fminf(lo.y, c.y); lo.z = fminf(lo.z, c.z);
+                            hi.x = fmaxf(hi.x, c.x); hi.y = fmaxf(hi.y, c.y); hi.z = fmaxf(hi.z, c.z);
+                            lo.w = fmaxf(lo.w, c.w);
+                            hi.w = fmaxf(hi.w, 1.0f + fabsf(c.x) + fabsf(c.y) + fabsf(c.z));
                         }
+                        S.blocks[2 * b] = lo;
+                        S.blocks[2 * b + 1] = hi;
+                    }
+                    for (int j = lane; j < nSt; j += team) S.segCount[j] = 0;
+                    teamSync(team, teamIdx);
+                    countSelfByBlocks(V, S, nSt, R.selfGap, table, lane, team, touching);
+                    teamSync(team, teamIdx);
+                    int total = 0;
+                    if (*touching) {  // team-uniform: one shared word read after the barrier
+                        for (int j = lane; j < nSt; j += team) S.segStart[j] = S.segCount[j];
+                        teamSync(team, teamIdx);
+                        total = teamExclusiveScan(S.segStart, nSt, lane, team, teamIdx, partial);
+                    }
+                    const int live = total < R.selfCapacity ? total : R.selfCapacity;
+                    if (lane == 0) {
+                        *S.live = live;
+                        if (total > R.selfCapacity) *S.overflow += total - R.selfCapacity;
+                    }
+                    if (live > 0) {
+                        // ---- fill, in the reference's order: its hash buckets ----
+                        for (int t = lane; t <= table; t += team) S.cellStart[t] = 0;
+                        for (int c = lane; c < live; c += team) S.pool[c].seg = -1;
+                        teamSync(team, teamIdx);
+                        for (int j = lane; j < nSt; j += team) {
+                            const float4 c = S.centres[j];
+                            const int h0 = int(hashCell(cellCoord(c.x, cell), cellCoord(c.y, cell),
+                                                        cellCoord(c.z, cell), table));
+                            S.cellOf[j] = h0;
+                            atomicAdd(&S.cellStart[h0], 1);
+                        }
+                        teamSync(team, teamIdx);
+                        // counts -> starts: cellStart[t] = first slot of bucket t,
+                        // cellStart[table] = segment count (the reference's offsets)
+                        teamExclusiveScan(S.cellStart, table + 1, lane, team, teamIdx, partial);
+                        for (int t = lane; t < table; t += team) cursor[t] = S.cellStart[t];
+                        teamSync(team, teamIdx);
+                        // stable placement, one warp walking segments in order
+                        if (lane < 32) {
+                            for (int j0 = 0; j0 < nSt; j0 += 32) {
+                                const int j = j0 + lane;
+                                const bool valid = j < nSt;
+                                const int c = valid ? S.cellOf[j] : -1 - lane;
+                                const unsigned peers = __match_any_sync(0xffffffffu, c);
+                                const int rank = __popc(peers & ((1u << lane) - 1u));
+                                const int start = valid ? cursor[c] : 0;
+                                __syncwarp();
+                                if (valid) {
+                                    S.sorted[start + rank] = j;
+                                    if (rank == 0) cursor[c] = start + __popc(peers);
+                                }
+                                __syncwarp();
+                            }
+                        }
+                        teamSync(team, teamIdx);
+                        for (int j = lane; j < nSt; j += team)
+                            if (S.segCount[j] > 0 && S.segStart[j] < R.selfCapacity)
+                                querySelfSegment<true>(V, S, j, nSt, R.selfGap, table, R.selfCapacity,
+                                                       R.selfFriction, true);
+                        // every thread is done reading the hash (sorted) before
+                        // cellOf and sorted (2 nSt >= nP ints) are reused below
+                        teamSync(team, teamIdx);
+                        for (int i = lane; i < nP; i += team) S.cellOf[i] = 0;
+                        teamSync(team, teamIdx);
+                        if (lane == 0) {
+                            int kept = live;
+                            *numLevels = buildProjectionLevels(S.pool, live, nP, S.cellOf, lvlOf, lvlOrder,
+                                                               lvlStart, &kept);
+                            if (kept != live) {
+                                // an entry indexed outside the rod or left unwritten:
+                                // keep the valid prefix and report it, never touch
+                                // memory with it
+                                *S.live = kept;
+                                if (A.errors) atomicOr(A.errors + r, 1);
+                            }
+                        }
+                    } else if (lane == 0) {
+                        *numLevels = 0;
                     }
                 } else if (lane == 0) {
-                    *numLevels = 0;
+                    for (int c = 0; c < *S.live; ++c) {
+                        S.pool[c].lambdaN = 0.0f;
+                        S.pool[c].applied = 0.0f;
+                    }
                 }
-            } else if (lane == 0) {
-                for (int c = 0; c < *S.live; ++c) {
-                    S.pool[c].lambdaN = 0.0f;
-                    S.pool[c].applied = 0.0f;
-                }
+                teamSync(team, teamIdx);
             }
+            for (int i = lane; i < nP; i += team) predictParticle<COMP>(V, i, h, g);
+            for (int j = lane; j < nS; j += team) predictFrame(V, j, h);
             teamSync(team, teamIdx);
-        }
-        for (int i = lane; i < nP; i += team) predictParticle<COMP>(V, i, h, g);
-        for (int j = lane; j < nS; j += team) predictFrame(V, j, h);
-        teamSync(team, teamIdx);
 
-        for (int it = 0; it < A.iterations; ++it) {
-            for (int c = 0; c < T.sColors; ++c) {
-                for (int ci = sCol[c] + lane; ci < sCol[c + 1]; ci += team)
-                    projectStretchOne<COMP>(V, sOrder[ci], invH2);
-                teamSync(team, teamIdx);
-            }
-            for (int c = 0; c < T.bColors; ++c) {
-                for (int ci = bCol[c] + lane; ci < bCol[c + 1]; ci += team)
-                    projectBendOne(V, bOrder[ci], invH2);
-                teamSync(team, teamIdx);
-            }
-            if (V.numPrims > 0) {
-                for (int i = lane; i < nP; i += team) projectSlots<COMP, FP64>(V, i, *primMask);
-                teamSync(team, teamIdx);
-            }
-            if (self) {
-                // level by level: contacts of one level share no particle, and
-                // every earlier contact a contact shares a particle with sits in
-                // a lower level -- the serial pool order's result, bit for bit
-                const int nl = *numLevels;
-                for (int l = 0; l < nl; ++l) {
-                    for (int c = lvlStart[l] + lane; c < lvlStart[l + 1]; c += team)
-                        projectSelf<COMP>(V, S.pool[lvlOrder[c]]);
+            for (int it = 0; it < A.iterations; ++it) {
+                // a chain coloured even/odd: constraint k of colour c is
+                // k = 2 i + c with particles k, k+1 and frames k, k+1, so no
+                // index is loaded; same constraints, same arithmetic
+                if (T.chain && (T.evenOdd & 1)) {
+                    for (int c = 0; c < 2; ++c) {
+                        for (int k = 2 * lane + c; k < nSt; k += 2 * team)
+                            projectStretchAt<COMP>(V, k, k, k + 1, k, invH2);
+                        teamSync(team, teamIdx);
+                    }
+                } else {
+                    for (int c = 0; c < T.sColors; ++c) {
+                        for (int ci = sCol[c] + lane; ci < sCol[c + 1]; ci += team)
+                            projectStretchOne<COMP>(V, sOrder[ci], invH2);
+                        teamSync(team, teamIdx);
+                    }
+                }
+                if (T.chain && (T.evenOdd & 2)) {
+                    for (int c = 0; c < 2; ++c) {
+                        for (int k = 2 * lane + c; k < nB; k += 2 * team) {
+                            if (k < nSt - 1)
+                                projectBendAt(V, k, k, k + 1, invH2);
+                            else
+                                projectBendOne(V, k, invH2);  // a ghost frame's bend
+                        }
+                        teamSync(team, teamIdx);
+                    }
+                } else {
+                    for (int c = 0; c < T.bColors; ++c) {
+                        for (int ci = bCol[c] + lane; ci < bCol[c + 1]; ci += team)
+                            projectBendOne(V, bOrder[ci], invH2);
+                        teamSync(team, teamIdx);
+                    }
+                }
+                if (V.numPrims > 0) {
+                    for (int i = lane; i < nP; i += team) projectSlots<COMP, FP64>(V, i, *primMask);
                     teamSync(team, teamIdx);
                 }
+                if (self) {
+                    // level by level: contacts of one level share no particle, and
+                    // every earlier contact a contact shares a particle with sits in
+                    // a lower level -- the serial pool order's result, bit for bit
+                    const int nl = *numLevels;
+                    for (int l = 0; l < nl; ++l) {
+                        for (int c = lvlStart[l] + lane; c < lvlStart[l + 1]; c += team)
+                            projectSelf<COMP>(V, S.pool[lvlOrder[c]]);
+                        teamSync(team, teamIdx);
+                    }
+                }
             }
+
+            for (int i = lane; i < nP; i += team) finishParticle<COMP>(V, i, h, A.linDecay);
+            for (int j = lane; j < nS; j += team) finishFrame(V, j, h, A.angDecay);
+            teamSync(team, teamIdx);
         }
 
-        for (int i = lane; i < nP; i += team) finishParticle<COMP>(V, i, h, A.linDecay);
-        for (int j = lane; j < nS; j += team) finishFrame(V, j, h, A.angDecay);
-        teamSync(team, teamIdx);
-    }
+        // ---- per-step bookkeeping ----
+        if (lane == 0) {
+            if (self) A.selfOverflow[r] += *S.overflow;
+            if (A.hold) {
+                DHold& H = A.hold[r];
+                if (H.particle >= 0 && H.particle < nP) {
+                    H.steps += 1;
+                    if (A.holdInterval > 0 && H.steps % A.holdInterval == 0) {
+                        double z = double(V.x[H.particle].z);
+                        if (COMP) z -= double(V.xComp[H.particle].z);
+                        const double rise = z - H.startZ;
+                        if (rise > H.maxRise) H.maxRise = rise;
+                    }
+                }
+            }
+        }
+        tRod += double(A.dt);
+    }  // steps of this launch
 
     // ---- stage out and outputs ----
     {
         float4* gx = A.x + R.pOff;
+        float4* gv = A.v + R.pOff;
         float4* gc = A.xComp + R.pOff;
         for (int i = lane; i < nP; i += team) {
             gx[i] = V.x[i];
+            gv[i] = V.v[i];
             if (COMP) gc[i] = V.xComp[i];
         }
         float4* gq = A.q + R.sOff;
-        for (int j = lane; j < nS; j += team) gq[j] = V.q[j];
+        float4* gw = A.omega + R.sOff;
+        for (int j = lane; j < nS; j += team) {
+            gq[j] = V.q[j];
+            gw[j] = V.omega[j];
+        }
     }
     if (V.numPrims > 0 && A.contactState) {
         const int slots = nP * V.numPrims;
@@ -376,23 +563,8 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
         for (int c = lane; c < live; c += team) A.selfPairs[R.poolOff + c] = S.pool[c].seg;
     }
     if (lane == 0) {
-        if (self) {
-            A.selfCount[r] = *S.live;
-            A.selfOverflow[r] += *S.overflow;
-        }
-        A.rodTime[r] += double(A.dt);
-        if (A.hold) {
-            DHold& H = A.hold[r];
-            if (H.particle >= 0 && H.particle < nP) {
-                H.steps += 1;
-                if (A.holdInterval > 0 && H.steps % A.holdInterval == 0) {
-                    double z = double(V.x[H.particle].z);
-                    if (COMP) z -= double(V.xComp[H.particle].z);
-                    const double rise = z - H.startZ;
-                    if (rise > H.maxRise) H.maxRise = rise;
-                }
-            }
-        }
+        if (self) A.selfCount[r] = *S.live;
+        A.rodTime[r] = tRod;
     }
 }
 
@@ -450,8 +622,8 @@ cudaError_t launchBatchedStep(const DArgs& a, const BatchedPlan& p, int precisio
     return fp64 ? launchB<false, true>(a, p, s) : launchB<false, false>(a, p, s);
 }
 
-cudaError_t batchedReserveSmem(size_t bytes) {
-    const int b = static_cast<int>(bytes);
+namespace {
+cudaError_t setMaxDynamicSmem_batched(int b) {
     cudaError_t e;
     if ((e = cudaFuncSetAttribute(kBatchedStep<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b)))
         return e;
@@ -460,6 +632,25 @@ cudaError_t batchedReserveSmem(size_t bytes) {
     if ((e = cudaFuncSetAttribute(kBatchedStep<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b)))
         return e;
     return cudaFuncSetAttribute(kBatchedStep<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+}
+}  // namespace
+
+// The attribute belongs to the kernel, not to a batch: it only ever grows
+// (per device), so a later, smaller plan never shrinks what an earlier batch
+// launches with.
+cudaError_t batchedReserveSmem(size_t bytes) {
+    static std::mutex mu;
+    static int reserved[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> g(mu);
+    const int want = static_cast<int>(bytes);
+    if (want <= reserved[dev]) return cudaSuccess;
+    e = setMaxDynamicSmem_batched(want);
+    if (e == cudaSuccess) reserved[dev] = want;
+    return e;
 }
 
 cudaError_t batchedOccupancy(int threads, size_t smem, int* perSm) {

@@ -173,6 +173,24 @@ void makeTemplate(const rp_rod_desc* d, TemplateHost& h) {
     h.order.insert(h.order.end(), order.begin(), order.end());
     h.colorStart.insert(h.colorStart.end(), cs.begin(), cs.end());
     T.chain = isChain(d);
+    // two colours holding the even and the odd constraints in ascending order:
+    // the kernel can then compute a constraint's index instead of loading it
+    auto evenOdd = [](const std::vector<int>& ord, const std::vector<int>& starts, int n) {
+        const int half = (n + 1) / 2;
+        if (n < 2 || starts.size() != 3 || starts[0] != 0 || starts[1] != half || starts[2] != n) return false;
+        for (int i = 0; i < n; ++i)
+            if (ord[i] != (i < half ? 2 * i : 2 * (i - half) + 1)) return false;
+        return true;
+    };
+    T.evenOdd = (evenOdd(std::vector<int>(h.order.begin(), h.order.begin() + d->num_stretch),
+                         std::vector<int>(h.colorStart.begin(), h.colorStart.begin() + T.sColors + 1),
+                         d->num_stretch)
+                     ? 1
+                     : 0) |
+                (evenOdd(std::vector<int>(h.order.begin() + T.bOrderOff, h.order.end()),
+                         std::vector<int>(h.colorStart.begin() + T.bColorOff, h.colorStart.end()), d->num_bend)
+                     ? 2
+                     : 0);
 }
 
 int teamThreads(int nSt, int pairsPerThread) {

@@ -35,7 +35,8 @@ struct DTemplate {
     int32_t sColors, bColors;
     int32_t chain;                 // 1: stretch k = (k, k+1, frame k) for all k, bends of
                                    // real frames (k, k+1) for k < nSt-1, ghosts after
-    int32_t pad;
+    int32_t evenOdd;               // bit 0: stretch colour order is {0,2,4..},{1,3,5..};
+                                   // bit 1: the same for the bends
 };
 
 // One rod of the batch.
@@ -156,6 +157,7 @@ struct DArgs {
     int32_t precision;
     float dt;
     int32_t maxPrims;
+    int32_t stepsPerLaunch;  // batched kernel: whole steps per launch (<= 0 means 1)
 };
 
 }  // namespace rp

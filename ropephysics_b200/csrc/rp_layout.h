@@ -3,21 +3,22 @@
 //
 // Per rod, in bytes (16-byte aligned sections). The full layout (plain
 // kernel) stages every state array, as the reference's fused kernel does. The
-// lean layout (batched kernel) keeps only what the colour sweeps and the
-// self-collision broad phase read many times per substep -- positions and
-// their start-of-substep copies, frames, multipliers, the hash -- and leaves
-// in global memory what is touched once or twice per substep (velocities,
-// angular velocities, loads, qPrev) or only when a contact is live (world
-// contact slots of primitives that survive the per-rod cull, the self-contact
-// pool); those stay L1/L2-resident.
-//   frames     q [, qPrev, omega, torque]            16 x nS each
-//   particles  x, xPrev [, v, force, kin], xComp     16 x nP each (xComp: full,
+// lean layout (batched kernel) keeps what every substep reads and writes --
+// positions and their start-of-substep copies, frames, velocities, angular
+// velocities, multipliers, the hash -- and leaves in global memory what a
+// step only reads (loads, kinematic velocities), what is touched once per
+// substep (qPrev) or only when a contact is live (world contact slots of
+// primitives that survive the per-rod cull, the self-contact pool); those
+// stay L1/L2-resident.
+//   frames     q [, qPrev], omega [, torque]         16 x nS each
+//   particles  x, xPrev, v [, force, kin], xComp     16 x nP each (xComp: full,
 //                                                    or lean with compensation)
 //   lambdas    stretch, bend                         16 x (nSt + nB)
 //   slots      [world contacts]                      32 x nP x numPrims
 //   misc       kMiscBytes (below)
 //   self       centres 16 nSt, ints 16 nSt, hash + cursor 2 x 4 (table + 1),
-//              [pool 64 x capacity], projection levels 3 x 4 (capacity + 1)
+//              [pool 64 x capacity], projection levels 3 x 4 (capacity + 1),
+//              [chain-block bounds 32 x ceil(nSt / 8)] (lean)
 #pragma once
 
 #include <cstdint>
@@ -35,13 +36,14 @@ struct RodLayout {
     int32_t x, xPrev, v, force, kin, xComp;
     int32_t lamS, lamB;
     int32_t slots;
-    int32_t centres, selfInt, misc, hash, pool, levels;
+    int32_t centres, selfInt, misc, hash, pool, levels, blocks;
     int32_t bytes;
 };
 
 // Per-rod scalars and team reduction scratch, as 32-bit words:
 //   [0] cell size  [1] live pool entries  [2] overflow  [3] projection levels
 //   [4..11] per-warp scan partials  [12..13] primitive mask (64 bits)
+//   [14] a self-contact pair touches this substep (batched)
 //   [16..79] per-warp reduction rows (8 warps x 8 floats)
 constexpr int32_t kMiscBytes = 320;
 
@@ -60,14 +62,14 @@ RP_HD inline RodLayout rodLayout(int32_t nP, int32_t nS, int32_t nSt, int32_t nB
     }
     L.x = o;      o += 16 * nP;
     L.xPrev = o;  o += 16 * nP;
+    L.omega = o;  o += 16 * nS;
+    L.v = o;      o += 16 * nP;
     if (!lean) {
-        L.omega = o;  o += 16 * nS;
         L.torque = o; o += 16 * nS;
-        L.v = o;      o += 16 * nP;
         L.force = o;  o += 16 * nP;
         L.kin = o;    o += 16 * nP;
     } else {
-        L.omega = L.torque = L.v = L.force = L.kin = -1;
+        L.torque = L.force = L.kin = -1;
     }
     if (!lean || comp) {
         L.xComp = o;  o += 16 * nP;
@@ -92,8 +94,14 @@ RP_HD inline RodLayout rodLayout(int32_t nP, int32_t nS, int32_t nSt, int32_t nB
             L.pool = -1;
         }
         L.levels = o;  o += rpAlign16(12 * (capacity + 1));
+        if (lean) {
+            L.blocks = o;  o += 32 * ((nSt + 7) / 8);
+        } else {
+            L.blocks = -1;
+        }
     } else {
         L.centres = L.selfInt = L.hash = L.pool = L.levels = o;
+        L.blocks = -1;
     }
     L.bytes = o;
     return L;

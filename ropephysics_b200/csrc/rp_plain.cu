@@ -14,6 +14,8 @@
 // self-contact projection on one thread) on purpose.
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "rp_launch.h"
 #include "rp_layout.h"
 #include "rp_step_common.cuh"
@@ -336,8 +338,8 @@ cudaError_t launchPlainStep(const DArgs& a, int gmem, int precision, int threads
                 : launchOne<false, false, false>(a, threads, smem, s);
 }
 
-cudaError_t plainReserveSmem(size_t bytes) {
-    const int b = static_cast<int>(bytes);
+namespace {
+cudaError_t setMaxDynamicSmem_plain(int b) {
     cudaError_t e;
     if ((e = cudaFuncSetAttribute(kPlainStep<false, false, false>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, b)) != cudaSuccess)
@@ -350,6 +352,25 @@ cudaError_t plainReserveSmem(size_t bytes) {
         return e;
     return cudaFuncSetAttribute(kPlainStep<false, true, true>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+}
+}  // namespace
+
+// The attribute belongs to the kernel, not to a batch: it only ever grows
+// (per device), so a later, smaller plan never shrinks what an earlier batch
+// launches with.
+cudaError_t plainReserveSmem(size_t bytes) {
+    static std::mutex mu;
+    static int reserved[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> g(mu);
+    const int want = static_cast<int>(bytes);
+    if (want <= reserved[dev]) return cudaSuccess;
+    e = setMaxDynamicSmem_plain(want);
+    if (e == cudaSuccess) reserved[dev] = want;
+    return e;
 }
 
 cudaError_t launchObserve(const DArgs& a, int compensated, cudaStream_t s) {

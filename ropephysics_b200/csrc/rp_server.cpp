@@ -112,6 +112,10 @@ constexpr int64_t kUnitBytes[NUNITS] = {
     int64_t(sizeof(rp::DPrim)),                  // PRIM
 };
 
+// Whole steps per server launch (fewer host round trips; admission happens
+// between launches).
+constexpr int kMaxStepsPerLaunch = 4;
+
 double nowS() {
     using namespace std::chrono;
     return duration<double>(steady_clock::now().time_since_epoch()).count();
@@ -383,6 +387,12 @@ void rp_server::loop() {
         A.contactInterval = p.contact_interval > 0 ? p.contact_interval : 1;
         A.dt = p.dt;
         A.precision = cfg.precision;
+        // whole steps in this launch: up to kMaxStepsPerLaunch, never past a
+        // running request's horizon (new requests join at launch boundaries)
+        int stepsNow = kMaxStepsPerLaunch;
+        for (auto& rq : running) stepsNow = std::min(stepsNow, rq->steps - rq->stepsDone);
+        stepsNow = std::max(stepsNow, 1);
+        A.stepsPerLaunch = stepsNow;
         rp::BatchedPlan bp;
         bp.groups = dGroups;
         bp.numGroups = groupsN;
@@ -398,27 +408,23 @@ void rp_server::loop() {
             workerError = std::string("step failed: ") + cudaGetErrorString(e);
             break;
         }
-        ++st.steps_launched;
+        st.steps_launched += stepsNow;
         // ---- retire ----
         bool any = false;
         for (auto& rq : running) {
-            if (++rq->stepsDone < rq->steps) continue;
+            rq->stepsDone += stepsNow;
+            if (rq->stepsDone < rq->steps) continue;
             any = true;
-            rq->result.assign(size_t(3 * rq->particles), 0.0f);
-            std::vector<float4> xs;
-            size_t at = 0;
-            for (int i = 0; i < rq->numRods && !e; ++i) {
-                const int nP = rq->rodNP[i];
-                xs.resize(nP);
-                e = cudaMemcpy(xs.data(), a.x + hRods[rq->rodIds[i]].pOff, nP * sizeof(float4),
-                               cudaMemcpyDeviceToHost);
-                for (int j = 0; j < nP; ++j, ++at) {
-                    rq->result[3 * at] = xs[j].x;
-                    rq->result[3 * at + 1] = xs[j].y;
-                    rq->result[3 * at + 2] = xs[j].z;
-                }
-            }
+            // a request's particles are one contiguous range, rods in order
+            std::vector<float4> xs(size_t(rq->counts[SP]));
+            e = cudaMemcpy(xs.data(), a.x + rq->offs[SP], xs.size() * sizeof(float4), cudaMemcpyDeviceToHost);
             if (e) break;
+            rq->result.assign(size_t(3 * rq->particles), 0.0f);
+            for (size_t j = 0; j < xs.size(); ++j) {
+                rq->result[3 * j] = xs[j].x;
+                rq->result[3 * j + 1] = xs[j].y;
+                rq->result[3 * j + 2] = xs[j].z;
+            }
             for (int u = 0; u < NUNITS; ++u) arena[u].release(rq->offs[u], rq->counts[u]);
             st.resident_bytes -= rq->residentBytes;
             rq->state = RP_REQUEST_DONE;

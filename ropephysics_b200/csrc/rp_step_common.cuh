@@ -87,9 +87,10 @@ __device__ __forceinline__ V3 dispOf(const RodView& V, int i) {
 
 // ---------------------------------------------------------------- constraints
 
+// Stretch constraint k between particles i0, i1 and frame j (the caller
+// passes sP0[k], sP1[k], sSeg[k], or k, k+1, k for a chain).
 template <bool COMP>
-__device__ __forceinline__ void projectStretchOne(const RodView& V, int k, float invH2) {
-    const int i0 = V.sP0[k], i1 = V.sP1[k], j = V.sSeg[k];
+__device__ __forceinline__ void projectStretchAt(const RodView& V, int k, int i0, int i1, int j, float invH2) {
     const float w0 = V.invMass[i0], w1 = V.invMass[i1];
     const V3 iI = v3(V.invInertia[j]);
     if (w0 == 0.0f && w1 == 0.0f && norm2(iI) == 0.0f) return;
@@ -120,8 +121,14 @@ __device__ __forceinline__ void projectStretchOne(const RodView& V, int k, float
     if (norm2(iI) > 0.0f) V.q[j] = f4(applyBodyDelta(q, cwise(iI, cross(dL, u))));
 }
 
-__device__ __forceinline__ void projectBendOne(const RodView& V, int k, float invH2) {
-    const int a = V.bA[k], b = V.bB[k];
+template <bool COMP>
+__device__ __forceinline__ void projectStretchOne(const RodView& V, int k, float invH2) {
+    projectStretchAt<COMP>(V, k, V.sP0[k], V.sP1[k], V.sSeg[k], invH2);
+}
+
+// Bend/twist constraint k between frames a and b (bA[k], bB[k], or k, k+1
+// for a chain's real frames).
+__device__ __forceinline__ void projectBendAt(const RodView& V, int k, int a, int b, float invH2) {
     const V3 iIa = v3(V.invInertia[a]), iIb = v3(V.invInertia[b]);
     if (norm2(iIa) == 0.0f && norm2(iIb) == 0.0f) return;
 
@@ -155,6 +162,10 @@ __device__ __forceinline__ void projectBendOne(const RodView& V, int k, float in
         const V3 g = (dL * p.w - cross(im(p), dL)) * (1.0f / lbar);
         V.q[b] = f4(applyBodyDelta(qb, cwise(iIb, g)));
     }
+}
+
+__device__ __forceinline__ void projectBendOne(const RodView& V, int k, float invH2) {
+    projectBendAt(V, k, V.bA[k], V.bB[k], invH2);
 }
 
 // ---------------------------------------------------------------- world contacts
@@ -331,7 +342,25 @@ struct SelfScratch {
     float* cellSize;   // 1
     int32_t* live;     // 1
     int32_t* overflow; // 1
+    float4* blocks;    // chain blocks of 8 segments: {lo, max half}, {hi, max 1 + |c|_1}
 };
+
+// Narrow phase of one segment pair: closest points (u on a, w on b), their
+// difference, its length and the separation dist - 2r. Not inlined, so every
+// caller -- the counting broad phases and the filling pass -- runs one
+// compiled body and decides contacts identically.
+struct SegPair {
+    float u, w, dist, separation;
+    V3 delta;
+};
+static __device__ __noinline__ SegPair segmentPairNarrow(V3 a0, V3 a1, V3 b0, V3 b1, float twoR) {
+    SegPair r;
+    closestPointsBetweenSegments(a0, a1, b0, b1, r.u, r.w);
+    r.delta = (a0 + (a1 - a0) * r.u) - (b0 + (b1 - b0) * r.w);
+    r.dist = norm(r.delta);
+    r.separation = r.dist - twoR;
+    return r;
+}
 
 // Contacts of segment j with later segments, in the reference's candidate
 // order (3x3x3 cells z/y/x, bucket order within a cell). fill = false counts
@@ -372,12 +401,10 @@ __device__ __forceinline__ void querySelfSegment(const RodView& V, const SelfScr
                             if (ddx * ddx + ddy * ddy + ddz * ddz > lim * lim) continue;
                         }
                         const V3 b0 = v3(V.x[V.sP0[k]]), b1 = v3(V.x[V.sP1[k]]);
-                        float u, w;
-                        closestPointsBetweenSegments(a0, a1, b0, b1, u, w);
-                        const V3 delta = (a0 + (a1 - a0) * u) - (b0 + (b1 - b0) * w);
-                        const float dist = norm(delta);
-                        const float separation = dist - twoR;
-                        if (separation >= 0.0f) continue;
+                        const SegPair P = segmentPairNarrow(a0, a1, b0, b1, twoR);
+                        if (P.separation >= 0.0f) continue;
+                        const float u = P.u, w = P.w, dist = P.dist, separation = P.separation;
+                        const V3 delta = P.delta;
                         const int slot = fill ? S.segStart[j] + count : 0;
                         ++count;
                         if (!fill || slot >= capacity) continue;
@@ -415,9 +442,9 @@ __device__ __forceinline__ void querySelfSegment(const RodView& V, const SelfScr
 // computes. `last` holds one zeroed int per particle; `lvlOf` one int per
 // contact. Fills order[live] (contacts grouped by level, pool order within a
 // level) and start[levels + 1]; returns the number of levels. Entries whose
-// particle indices fall outside [0, nP) are never dereferenced: the pool is
-// cut before the first of them and *kept says how many entries remain. One
-// thread.
+// particle indices fall outside [0, nP), or marked unwritten (seg == -1), are
+// never dereferenced: the pool is cut before the first of them and *kept says
+// how many entries remain. One thread.
 __device__ __forceinline__ int buildProjectionLevels(const DSelf* pool, int live, int nP, int32_t* last,
                                                      int32_t* lvlOf, int32_t* order, int32_t* start,
                                                      int* kept) {
@@ -425,6 +452,7 @@ __device__ __forceinline__ int buildProjectionLevels(const DSelf* pool, int live
         const DSelf& k = pool[c];
         bool ok = true;
         for (int m = 0; m < 4; ++m) ok = ok && k.idx[m] >= 0 && k.idx[m] < nP;
+        ok = ok && k.seg != -1;  // -1: a slot the filling pass left unwritten
         if (!ok) {
             live = c;
             break;

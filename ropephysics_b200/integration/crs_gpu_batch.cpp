@@ -13,7 +13,12 @@
 // Strategy mapping: kFused -> RP_STRATEGY_BATCHED (the persistent form; its
 // results equal the one-rod-per-CTA step bit for bit), kMultiKernel ->
 // RP_STRATEGY_MULTI_KERNEL (state in global memory, any rod length).
+//
+// The reference API has no precision setting; the environment variable
+// RP_B200_PRECISION (an rp_precision flag word, default 0 = the reference's
+// FP32 operation order) selects one for every batch this binding creates.
 #include <cstdio>
+#include <cstdlib>
 #include <string>
 #include <vector>
 
@@ -147,6 +152,13 @@ bool Batch::create(const Rod& prototype, int numRods, Strategy strategy, const C
         report("create");
         delete im;
         return false;
+    }
+    if (const char* flags = std::getenv("RP_B200_PRECISION")) {
+        if (rp_batch_set_precision(im->batch, int32_t(std::atoi(flags))) != RP_OK) {
+            report("set_precision");
+            delete im;  // destroys the batch
+            return false;
+        }
     }
     impl_ = im;
     numRods_ = numRods;

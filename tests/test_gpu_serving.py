@@ -86,15 +86,32 @@ def test_budget_admission_and_queueing():
         sizes.append(probe.info(rid)["resident_bytes"])
     probe.drain(300)
     probe.close()
-    # every request fits alone, no two fit together
-    budget = sum(sorted(sizes)[:2]) - 1
-    assert budget >= max(sizes) and budget >= (1 << 20)
+    # the smallest budget, in steps of 1/8, whose arenas take the largest
+    # request: every request fits alone, and the six cannot all be resident
+    # at once, so later ones wait for earlier ones to retire
+    big = reqs[int(np.argmax(sizes))]
+    budget = max(max(sizes), 1 << 20)
+    for _ in range(64):
+        probe = rp.Server(budget, PARAMS)
+        try:
+            submit(probe, big)
+            fits = True
+        except rp.RopeError as e:
+            assert e.status == 6
+            fits = False
+        probe.drain(300)
+        probe.close()
+        if fits:
+            break
+        budget = int(budget * 1.125)
+    assert fits
     server = rp.Server(budget, PARAMS)
     ids = [submit(server, r) for r in reqs]
     server.drain(600)
     st = server.stats()
     assert st["completed"] == len(reqs)
     assert st["peak_resident_bytes"] <= budget
+    assert st["peak_resident_bytes"] < sum(sizes)  # never all resident at once
     infos = [server.info(i) for i in ids]
     # FIFO: admissions in submission order, and some waited for an earlier retire
     admits = [i["admit_s"] for i in infos]

@@ -208,3 +208,28 @@ def test_op_count_oracle_reproduces_double():
     assert np.array_equal(a.x, b.x)
     ops = oc.op_counts()
     assert ops["add"] > 0 and ops["mul"] > 0 and ops["div"] > 0 and ops["sqrt"] > 0
+
+
+def test_flops_per_segment_substep_match_bench():
+    """The bench's algorithmic FLOPs per segment-substep (add, sub, mul, div,
+    sqrt) are the op-counting oracle's count for a pinned 64-segment rod at
+    dt 1/60 with 20 substeps, free and with a floor plane."""
+    import bench
+    from oracle import Context, Oracle, Primitive as OP, World as OW
+    oc = Oracle("count")
+    p = Params(dt=1 / 60, substeps=20, iterations=1)
+
+    def per_seg_substep(world):
+        r = oc.straight(64, 1.0, youngs=1e8, poisson=0.3, density=1100, radius=5e-3, direction=(0, 0, -1))
+        oc.pin(r, 0)
+        ctx = Context(dtype=np.float64) if world else None
+        oc.step(r, p, world=world, ctx=ctx, steps=1)
+        oc.op_reset()
+        oc.step(r, p, world=world, ctx=ctx, steps=1)
+        c = oc.op_counts()
+        return sum(c[k] for k in ("add", "mul", "div", "sqrt")) / (64 * 20)
+
+    # the bench quotes them to one decimal
+    assert per_seg_substep(None) == pytest.approx(bench.FLOPS_PER_SEG_SUBSTEP["uneven"], abs=0.05)
+    floor = OW([OP.plane((0, 0, -1.2), (0, 0, 1), 0.5)])
+    assert per_seg_substep(floor) == pytest.approx(bench.FLOPS_PER_SEG_SUBSTEP["grid"], abs=0.05)
