@@ -381,6 +381,7 @@ static rp_status createImpl(const rp_rod_desc* const* rods, int numRods, const r
     ALLOC(A.force, float4, P);
     ALLOC(A.kinVel, float4, P);
     ALLOC(A.xComp, float4, P);
+    ALLOC(A.qComp, float4, S);
     ALLOC(A.q, float4, S);
     ALLOC(A.omega, float4, S);
     ALLOC(A.torque, float4, S);
@@ -768,6 +769,7 @@ rp_status rp_batch_set_precision(rp_batch* b, int32_t flags) {
     if ((flags & RP_PRECISION_COMPENSATED) != (b->precision & RP_PRECISION_COMPENSATED)) {
         // entering or leaving compensated mode: the compensation starts at zero
         RP_CUDA(cudaMemsetAsync(b->a.xComp, 0, size_t(b->totalP) * sizeof(float4), b->stream));
+        RP_CUDA(cudaMemsetAsync(b->a.qComp, 0, size_t(b->totalS) * sizeof(float4), b->stream));
         b->precision = flags;
         // the batched layout keeps the compensation in shared memory
         if (b->strategy == RP_STRATEGY_BATCHED) {
@@ -842,6 +844,7 @@ struct StateSnapshot {
         add(A.x, P * 16);
         add(A.v, P * 16);
         add(A.xComp, P * 16);
+        add(A.qComp, S * 16);
         add(A.kinVel, P * 16);
         add(A.q, S * 16);
         add(A.omega, S * 16);
@@ -978,6 +981,8 @@ rp_status rp_batch_download(rp_batch* b, int32_t rod, rp_rod_desc* out) {
     RP_CUDA(cudaMemcpyAsync(c.data(), b->a.xComp + R.pOff, nP * sizeof(float4), cudaMemcpyDeviceToHost, b->stream));
     RP_CUDA(cudaMemcpyAsync(q.data(), b->a.q + R.sOff, nS * sizeof(float4), cudaMemcpyDeviceToHost, b->stream));
     RP_CUDA(cudaMemcpyAsync(w.data(), b->a.omega + R.sOff, nS * sizeof(float4), cudaMemcpyDeviceToHost, b->stream));
+    std::vector<float4> qc(nS, make_float4(0, 0, 0, 0));
+    RP_CUDA(cudaMemcpyAsync(qc.data(), b->a.qComp + R.sOff, nS * sizeof(float4), cudaMemcpyDeviceToHost, b->stream));
     rp_status st = syncBatch(b);
     if (st != RP_OK) return st;
     const bool comp = (b->precision & RP_PRECISION_COMPENSATED) != 0;
@@ -992,10 +997,10 @@ rp_status rp_batch_download(rp_batch* b, int32_t rod, rp_rod_desc* out) {
         }
     }
     for (int j = 0; j < nS; ++j) {
-        out->q[4 * j] = q[j].x;
-        out->q[4 * j + 1] = q[j].y;
-        out->q[4 * j + 2] = q[j].z;
-        out->q[4 * j + 3] = q[j].w;
+        out->q[4 * j] = double(q[j].x) - (comp ? double(qc[j].x) : 0.0);
+        out->q[4 * j + 1] = double(q[j].y) - (comp ? double(qc[j].y) : 0.0);
+        out->q[4 * j + 2] = double(q[j].z) - (comp ? double(qc[j].z) : 0.0);
+        out->q[4 * j + 3] = double(q[j].w) - (comp ? double(qc[j].w) : 0.0);
         if (out->omega) {
             out->omega[3 * j] = w[j].x;
             out->omega[3 * j + 1] = w[j].y;
@@ -1030,10 +1035,19 @@ rp_status rp_batch_download_frames(rp_batch* b, float* out, int64_t cap) {
     if (!b || !out) return fail(RP_ERR_INVALID, "batch or out is NULL");
     const size_t S = size_t(b->totalS);
     if (cap < int64_t(4 * S)) return fail(RP_ERR_INVALID, "capacity below 4 x total frames");
-    std::vector<float4> q(S);
+    std::vector<float4> q(S), c;
     RP_CUDA(cudaMemcpyAsync(q.data(), b->a.q, S * sizeof(float4), cudaMemcpyDeviceToHost, b->stream));
+    const bool comp = (b->precision & RP_PRECISION_COMPENSATED) != 0;
+    if (comp) {
+        c.resize(S);
+        RP_CUDA(cudaMemcpyAsync(c.data(), b->a.qComp, S * sizeof(float4), cudaMemcpyDeviceToHost, b->stream));
+    }
     rp_status st = syncBatch(b);
     if (st != RP_OK) return st;
+    if (comp)
+        for (size_t j = 0; j < S; ++j)
+            q[j] = make_float4(float(double(q[j].x) - c[j].x), float(double(q[j].y) - c[j].y),
+                               float(double(q[j].z) - c[j].z), float(double(q[j].w) - c[j].w));
     std::memcpy(out, q.data(), S * sizeof(float4));
     return RP_OK;
 }
@@ -1050,9 +1064,21 @@ static rp_status setLoadsImpl(rp_batch* b, int rod, const rp_rod_desc* s) {
     // fixed frames (zero inertia) take their orientation from the source:
     // how an end is driven, e.g. twisted (gpu_batch.cpp:386-389)
     const std::vector<char>& fixed = b->fixedFrame[R.tmpl];
+    // compensated precision: the driven frame's rounding error goes to qComp,
+    // so the imposed orientation is carried to FP64 accuracy
+    const bool comp = (b->precision & RP_PRECISION_COMPENSATED) != 0;
+    std::vector<float4> qc(nS, make_float4(0, 0, 0, 0));
+    for (int j = 0; j < nS && comp; ++j) {
+        const double* src = s->q + 4 * j;  // w, x, y, z
+        qc[j] = make_float4(float(double(q[j].x) - src[0]), float(double(q[j].y) - src[1]),
+                            float(double(q[j].z) - src[2]), float(double(q[j].w) - src[3]));
+    }
     for (int j = 0; j < nS; ++j)
-        if (fixed[j])
+        if (fixed[j]) {
             RP_CUDA(cudaMemcpyAsync(b->a.q + R.sOff + j, &q[j], sizeof(float4), cudaMemcpyHostToDevice, b->stream));
+            RP_CUDA(cudaMemcpyAsync(b->a.qComp + R.sOff + j, &qc[j], sizeof(float4), cudaMemcpyHostToDevice,
+                                    b->stream));
+        }
     return syncBatch(b);
 }
 
@@ -1063,16 +1089,38 @@ rp_status rp_batch_set_loads(rp_batch* b, int32_t rod, const rp_rod_desc* s) {
     return setLoadsImpl(b, rod, s);
 }
 
+// Compensation of freshly uploaded state: zero in reference order; with
+// compensated precision the rounding residual of each double input (float
+// value minus the double), so that value - compensation is the input exactly.
+static void uploadResiduals(const rp_batch* b, const rp_rod_desc* s, const float4* x, const float4* q,
+                            float4* xc, float4* qc) {
+    const bool comp = (b->precision & RP_PRECISION_COMPENSATED) != 0;
+    for (int i = 0; i < s->num_particles; ++i) {
+        const double* p = s->x + 3 * i;
+        xc[i] = comp ? make_float4(float(double(x[i].x) - p[0]), float(double(x[i].y) - p[1]),
+                                   float(double(x[i].z) - p[2]), 0.0f)
+                     : make_float4(0, 0, 0, 0);
+    }
+    for (int j = 0; j < s->num_frames; ++j) {
+        const double* p = s->q + 4 * j;  // w, x, y, z as q[j].x .. q[j].w
+        qc[j] = comp ? make_float4(float(double(q[j].x) - p[0]), float(double(q[j].y) - p[1]),
+                                   float(double(q[j].z) - p[2]), float(double(q[j].w) - p[3]))
+                     : make_float4(0, 0, 0, 0);
+    }
+}
+
 static rp_status uploadRodImpl(rp_batch* b, int rod, const rp_rod_desc* s) {
     const DRod& R = b->rods[rod];
     const int nP = b->tmplNP[rod], nS = b->tmplNS[rod];
-    std::vector<float4> x(nP), v(nP), q(nS), w(nS), z(nP, make_float4(0, 0, 0, 0));
+    std::vector<float4> x(nP), v(nP), q(nS), w(nS), xc(nP), qc(nS);
     packParticles(s, x.data(), v.data(), nullptr, nullptr);
     packFrames(s, q.data(), w.data(), nullptr);
+    uploadResiduals(b, s, x.data(), q.data(), xc.data(), qc.data());
     RP_CUDA(cudaMemcpyAsync(b->a.x + R.pOff, x.data(), nP * sizeof(float4), cudaMemcpyHostToDevice, b->stream));
     RP_CUDA(cudaMemcpyAsync(b->a.v + R.pOff, v.data(), nP * sizeof(float4), cudaMemcpyHostToDevice, b->stream));
-    RP_CUDA(cudaMemcpyAsync(b->a.xComp + R.pOff, z.data(), nP * sizeof(float4), cudaMemcpyHostToDevice, b->stream));
+    RP_CUDA(cudaMemcpyAsync(b->a.xComp + R.pOff, xc.data(), nP * sizeof(float4), cudaMemcpyHostToDevice, b->stream));
     RP_CUDA(cudaMemcpyAsync(b->a.q + R.sOff, q.data(), nS * sizeof(float4), cudaMemcpyHostToDevice, b->stream));
+    RP_CUDA(cudaMemcpyAsync(b->a.qComp + R.sOff, qc.data(), nS * sizeof(float4), cudaMemcpyHostToDevice, b->stream));
     RP_CUDA(cudaMemcpyAsync(b->a.omega + R.sOff, w.data(), nS * sizeof(float4), cudaMemcpyHostToDevice, b->stream));
     return setLoadsImpl(b, rod, s);
 }
@@ -1092,18 +1140,18 @@ rp_status rp_batch_upload(rp_batch* b, const rp_rod_desc* s) {
             return fail(RP_ERR_INVALID, "source does not have rod " + std::to_string(r) + "'s topology");
     }
     const size_t P = size_t(b->totalP), S = size_t(b->totalS);
-    std::vector<float4> hx(P), hv(P), hf(P), hk(P), hq(S), hw(S), ht(S);
+    std::vector<float4> hx(P), hv(P), hf(P), hk(P), hq(S), hw(S), ht(S), hxc(P), hqc(S);
     for (int r = 0; r < b->numRods; ++r) {
         const DRod& R = b->rods[r];
         packParticles(s, &hx[R.pOff], &hv[R.pOff], &hf[R.pOff], &hk[R.pOff]);
         packFrames(s, &hq[R.sOff], &hw[R.sOff], &ht[R.sOff]);
+        uploadResiduals(b, s, &hx[R.pOff], &hq[R.sOff], &hxc[R.pOff], &hqc[R.sOff]);
     }
     rp_status st;
     if ((st = b->upload(b->a.x, hx)) || (st = b->upload(b->a.v, hv)) || (st = b->upload(b->a.force, hf)) ||
         (st = b->upload(b->a.kinVel, hk)) || (st = b->upload(b->a.q, hq)) || (st = b->upload(b->a.omega, hw)) ||
-        (st = b->upload(b->a.torque, ht)))
+        (st = b->upload(b->a.torque, ht)) || (st = b->upload(b->a.xComp, hxc)) || (st = b->upload(b->a.qComp, hqc)))
         return st;
-    RP_CUDA(cudaMemsetAsync(b->a.xComp, 0, P * sizeof(float4), b->stream));
     return syncBatch(b);
 }
 

@@ -211,6 +211,7 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
     V.x = reinterpret_cast<float4*>(base + L.x);
     V.xPrev = reinterpret_cast<float4*>(base + L.xPrev);
     V.xComp = COMP ? reinterpret_cast<float4*>(base + L.xComp) : A.xComp + R.pOff;
+    V.qComp = COMP ? reinterpret_cast<float4*>(base + L.qComp) : A.qComp + R.sOff;
     // lean layout: loads and kinematic velocities stay in global memory
     V.v = reinterpret_cast<float4*>(base + L.v);
     V.force = A.force + R.pOff;
@@ -269,9 +270,11 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
         }
         const float4* gq = A.q + R.sOff;
         const float4* gw = A.omega + R.sOff;
+        const float4* gqc = A.qComp + R.sOff;
         for (int j = lane; j < nS; j += team) {
             V.q[j] = gq[j];
             V.omega[j] = gw[j];
+            if (COMP) V.qComp[j] = gqc[j];
         }
     }
 
@@ -457,8 +460,17 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
                 }
                 teamSync(team, teamIdx);
             }
-            for (int i = lane; i < nP; i += team) predictParticle<COMP>(V, i, h, g);
-            for (int j = lane; j < nS; j += team) predictFrame(V, j, h);
+            // the previous substep's velocity update runs here, fused with this
+            // substep's prediction: nothing between them reads v or omega,
+            // and each element's two updates stay with one thread
+            for (int i = lane; i < nP; i += team) {
+                if (sub > 0) finishParticle<COMP>(V, i, h, A.linDecay);
+                predictParticle<COMP>(V, i, h, g);
+            }
+            for (int j = lane; j < nS; j += team) {
+                if (sub > 0) finishFrame<COMP>(V, j, h, A.angDecay);
+                predictFrame<COMP>(V, j, h);
+            }
             teamSync(team, teamIdx);
 
             for (int it = 0; it < A.iterations; ++it) {
@@ -482,16 +494,16 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
                     for (int c = 0; c < 2; ++c) {
                         for (int k = 2 * lane + c; k < nB; k += 2 * team) {
                             if (k < nSt - 1)
-                                projectBendAt(V, k, k, k + 1, invH2);
+                                projectBendAt<COMP>(V, k, k, k + 1, invH2);
                             else
-                                projectBendOne(V, k, invH2);  // a ghost frame's bend
+                                projectBendOne<COMP>(V, k, invH2);  // a ghost frame's bend
                         }
                         teamSync(team, teamIdx);
                     }
                 } else {
                     for (int c = 0; c < T.bColors; ++c) {
                         for (int ci = bCol[c] + lane; ci < bCol[c + 1]; ci += team)
-                            projectBendOne(V, bOrder[ci], invH2);
+                            projectBendOne<COMP>(V, bOrder[ci], invH2);
                         teamSync(team, teamIdx);
                     }
                 }
@@ -512,10 +524,11 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
                 }
             }
 
-            for (int i = lane; i < nP; i += team) finishParticle<COMP>(V, i, h, A.linDecay);
-            for (int j = lane; j < nS; j += team) finishFrame(V, j, h, A.angDecay);
-            teamSync(team, teamIdx);
         }
+        // the step's last velocity update
+        for (int i = lane; i < nP; i += team) finishParticle<COMP>(V, i, h, A.linDecay);
+        for (int j = lane; j < nS; j += team) finishFrame<COMP>(V, j, h, A.angDecay);
+        teamSync(team, teamIdx);
 
         // ---- per-step bookkeeping ----
         if (lane == 0) {
@@ -548,9 +561,11 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
         }
         float4* gq = A.q + R.sOff;
         float4* gw = A.omega + R.sOff;
+        float4* gqc = A.qComp + R.sOff;
         for (int j = lane; j < nS; j += team) {
             gq[j] = V.q[j];
             gw[j] = V.omega[j];
+            if (COMP) gqc[j] = V.qComp[j];
         }
     }
     if (V.numPrims > 0 && A.contactState) {

@@ -124,6 +124,7 @@ struct DArgs {
     float4* omega;
     float4* torque;
     float4* xComp;  // Kahan compensation of x (RP_PRECISION_COMPENSATED)
+    float4* qComp;          // per frame: Kahan compensation of q (compensated precision)
 
     // scratch used in place of shared memory by the global-memory strategy
     float4* gxPrev;

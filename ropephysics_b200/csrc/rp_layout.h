@@ -13,6 +13,7 @@
 //   frames     q [, qPrev], omega [, torque]         16 x nS each
 //   particles  x, xPrev, v [, force, kin], xComp     16 x nP each (xComp: full,
 //                                                    or lean with compensation)
+//   frames     qComp                                 16 x nS (lean with compensation)
 //   lambdas    stretch, bend                         16 x (nSt + nB)
 //   slots      [world contacts]                      32 x nP x numPrims
 //   misc       kMiscBytes (below)
@@ -33,7 +34,7 @@ namespace rp {
 
 struct RodLayout {
     int32_t q, qPrev, omega, torque;
-    int32_t x, xPrev, v, force, kin, xComp;
+    int32_t x, xPrev, v, force, kin, xComp, qComp;
     int32_t lamS, lamB;
     int32_t slots;
     int32_t centres, selfInt, misc, hash, pool, levels, blocks;
@@ -75,6 +76,11 @@ RP_HD inline RodLayout rodLayout(int32_t nP, int32_t nS, int32_t nSt, int32_t nB
         L.xComp = o;  o += 16 * nP;
     } else {
         L.xComp = -1;
+    }
+    if (lean && comp) {
+        L.qComp = o;  o += 16 * nS;
+    } else {
+        L.qComp = -1;  // the plain kernel keeps it in global memory
     }
     L.lamS = o;   o += 16 * nSt;
     L.lamB = o;   o += 16 * nB;

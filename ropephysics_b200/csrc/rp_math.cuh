@@ -127,6 +127,9 @@ __device__ __forceinline__ Q4 conj(Q4 q) { return Q4{q.w, -q.x, -q.y, -q.z}; }
 __device__ __forceinline__ Q4 qadd(Q4 a, Q4 b) {
     return Q4{a.w + b.w, a.x + b.x, a.y + b.y, a.z + b.z};
 }
+__device__ __forceinline__ Q4 qsub(Q4 a, Q4 b) {
+    return Q4{a.w - b.w, a.x - b.x, a.y - b.y, a.z - b.z};
+}
 __device__ __forceinline__ Q4 qscale(Q4 q, float s) { return Q4{q.w * s, q.x * s, q.y * s, q.z * s}; }
 __device__ __forceinline__ float qdot(Q4 a, Q4 b) {
     return a.w * b.w + a.x * b.x + a.y * b.y + a.z * b.z;

@@ -141,6 +141,7 @@ __global__ void __launch_bounds__(128, 4) kPlainStep(DArgs A) {
         S.live = reinterpret_cast<int32_t*>(smem + L.misc) + 1;
         S.overflow = reinterpret_cast<int32_t*>(smem + L.misc) + 2;
     }
+    V.qComp = A.qComp + R.sOff;  // compensated frames: global in both forms
     S.sorted = S.cellOf + nSt;
     S.segCount = S.sorted + nSt;
     S.segStart = S.segCount + nSt;
@@ -227,7 +228,7 @@ __global__ void __launch_bounds__(128, 4) kPlainStep(DArgs A) {
             __syncthreads();
         }
         for (int i = tid; i < nP; i += nth) predictParticle<COMP>(V, i, h, g);
-        for (int j = tid; j < nS; j += nth) predictFrame(V, j, h);
+        for (int j = tid; j < nS; j += nth) predictFrame<COMP>(V, j, h);
         __syncthreads();
 
         for (int it = 0; it < A.iterations; ++it) {
@@ -238,7 +239,7 @@ __global__ void __launch_bounds__(128, 4) kPlainStep(DArgs A) {
             }
             for (int c = 0; c < T.bColors; ++c) {
                 for (int ci = bCol[c] + tid; ci < bCol[c + 1]; ci += nth)
-                    projectBendOne(V, bOrder[ci], invH2);
+                    projectBendOne<COMP>(V, bOrder[ci], invH2);
                 __syncthreads();
             }
             if (V.numPrims > 0) {
@@ -253,7 +254,7 @@ __global__ void __launch_bounds__(128, 4) kPlainStep(DArgs A) {
         }
 
         for (int i = tid; i < nP; i += nth) finishParticle<COMP>(V, i, h, A.linDecay);
-        for (int j = tid; j < nS; j += nth) finishFrame(V, j, h, A.angDecay);
+        for (int j = tid; j < nS; j += nth) finishFrame<COMP>(V, j, h, A.angDecay);
         __syncthreads();
     }
 

@@ -106,7 +106,7 @@ constexpr int64_t kUnitBytes[NUNITS] = {
     // order, group row
     int64_t(sizeof(rp::DRod)) + 8 + int64_t(sizeof(rp::DDrive)) + 8 + 4 + 8 + 4 + 16,
     5 * 16,                                      // SP   x, v, force, kin, xComp
-    4 * 16,                                      // SS   q, omega, torque, qPrev
+    5 * 16,                                      // SS   q, omega, torque, qPrev, qComp
     int64_t(sizeof(rp::DSlot)) + 1,              // SLOT slots + contact state
     int64_t(sizeof(rp::DSelf)) + 4,              // POOL pool + pair list
     int64_t(sizeof(rp::DPrim)),                  // PRIM
@@ -285,6 +285,7 @@ bool rp_server::admit(Request& rq) {
     P(a.omega, o[SS], rq.w);
     P(a.torque, o[SS], rq.t);
     if (!e) e = cudaMemsetAsync(a.xComp + o[SP], 0, size_t(rq.counts[SP]) * sizeof(float4), s);
+    if (!e) e = cudaMemsetAsync(a.qComp + o[SS], 0, size_t(rq.counts[SS]) * sizeof(float4), s);
     if (!e) e = cudaMemsetAsync(a.rodTime + o[ROD], 0, size_t(rq.numRods) * sizeof(double), s);
     if (!e) e = cudaMemsetAsync(a.selfOverflow + o[ROD], 0, size_t(rq.numRods) * sizeof(int32_t), s);
     if (!e) e = cudaMemsetAsync(a.selfCount + o[ROD], 0, size_t(rq.numRods) * sizeof(int32_t), s);
@@ -530,7 +531,7 @@ rp_status rp_server_create(const rp_server_config* cfg, rp_server** out) {
     ok = ok && s->dalloc(A.x, cap[SP]) && s->dalloc(A.v, cap[SP]) && s->dalloc(A.force, cap[SP]) &&
          s->dalloc(A.kinVel, cap[SP]) && s->dalloc(A.xComp, cap[SP]);
     ok = ok && s->dalloc(A.q, cap[SS]) && s->dalloc(A.omega, cap[SS]) && s->dalloc(A.torque, cap[SS]) &&
-         s->dalloc(A.gqPrev, cap[SS]);
+         s->dalloc(A.gqPrev, cap[SS]) && s->dalloc(A.qComp, cap[SS]);
     ok = ok && s->dalloc(A.gSlots, cap[SLOT]) && s->dalloc(A.contactState, cap[SLOT]);
     ok = ok && s->dalloc(A.gPool, cap[POOL]) && s->dalloc(A.selfPairs, cap[POOL]);
     ok = ok && s->dalloc(A.selfCount, cap[ROD]) && s->dalloc(A.selfOverflow, cap[ROD]) &&

@@ -35,6 +35,7 @@ struct RodView {
     float4* kin;
     float4* torque;
     float4* xComp;  // Kahan compensation (compensated precision only)
+    float4* qComp;  // frames' Kahan compensation (compensated precision only)
     DSlot* slots;
     // static template data (global memory, read-only)
     const float* invMass;
@@ -85,6 +86,46 @@ __device__ __forceinline__ V3 dispOf(const RodView& V, int i) {
     return COMP ? v3(V.xPrev[i]) : v3(V.x[i]) - v3(V.xPrev[i]);
 }
 
+// Compensated frames (RP_PRECISION_COMPENSATED). q holds the rounded frame
+// and qComp its running rounding error (true frame = q - qComp, the same
+// convention as positions); the qPrev slot holds e, the substep's accumulated
+// body rotation as the unit quaternion 1 + e, so small rotations accumulate
+// without being lost below FP32 spacing and the angular velocity needs no
+// cancelling difference of two frames.
+//
+// Frame j turned by the normalised body rotation (1, h)/|(1, h)| (h = half
+// the rotation vector, as applyBodyDelta and the frame prediction apply it).
+__device__ __forceinline__ void rotateFrameComp(const RodView& V, int j, V3 h) {
+    const float t = norm2(h);
+    const float s = sqrtf(1.0f + t);
+    const float invS = 1.0f / s;
+    // (1, h)/s - 1, with 1/s - 1 = -t / (s (1 + s)) free of cancellation
+    const Q4 eu = qmake(-t / (s * (1.0f + s)), h * invS);
+    const Q4 q = q4(V.q[j]);
+    const Q4 c = q4(V.qComp[j]);
+    const Q4 d = qsub(qmul(q, eu), qmul(c, eu));  // (q - c) (x) eu
+    const Q4 y = qsub(d, c);
+    const Q4 tq = qadd(q, y);
+    V.q[j] = f4(tq);
+    V.qComp[j] = f4(qsub(qsub(tq, q), y));
+    const Q4 e = q4(V.qPrev[j]);  // (1 + e)(1 + eu) = 1 + e + eu + e eu
+    V.qPrev[j] = f4(qadd(qadd(e, eu), qmul(e, eu)));
+}
+
+// Rescale frame j's true quaternion q - qComp to unit length in FP64 and
+// split it back into a rounded part and its error.
+__device__ __forceinline__ void renormalizeFrameComp(const RodView& V, int j) {
+    const float4 q = V.q[j], c = V.qComp[j];
+    const double a = double(q.x) - double(c.x), b = double(q.y) - double(c.y);
+    const double d = double(q.z) - double(c.z), e = double(q.w) - double(c.w);
+    const double inv = 1.0 / sqrt(a * a + b * b + d * d + e * e);
+    const double na = a * inv, nb = b * inv, nd = d * inv, ne = e * inv;
+    const float4 hi = make_float4(float(na), float(nb), float(nd), float(ne));
+    V.q[j] = hi;
+    V.qComp[j] = make_float4(float(double(hi.x) - na), float(double(hi.y) - nb), float(double(hi.z) - nd),
+                             float(double(hi.w) - ne));
+}
+
 // ---------------------------------------------------------------- constraints
 
 // Stretch constraint k between particles i0, i1 and frame j (the caller
@@ -118,7 +159,13 @@ __device__ __forceinline__ void projectStretchAt(const RodView& V, int k, int i0
     const V3 world = rotate(q, dL);
     addPos<COMP>(V, i0, -(world * (w0 / l)));
     addPos<COMP>(V, i1, world * (w1 / l));
-    if (norm2(iI) > 0.0f) V.q[j] = f4(applyBodyDelta(q, cwise(iI, cross(dL, u))));
+    if (norm2(iI) > 0.0f) {
+        const V3 theta = cwise(iI, cross(dL, u));
+        if (COMP)
+            rotateFrameComp(V, j, theta * 0.5f);
+        else
+            V.q[j] = f4(applyBodyDelta(q, theta));
+    }
 }
 
 template <bool COMP>
@@ -128,6 +175,7 @@ __device__ __forceinline__ void projectStretchOne(const RodView& V, int k, float
 
 // Bend/twist constraint k between frames a and b (bA[k], bB[k], or k, k+1
 // for a chain's real frames).
+template <bool COMP>
 __device__ __forceinline__ void projectBendAt(const RodView& V, int k, int a, int b, float invH2) {
     const V3 iIa = v3(V.invInertia[a]), iIb = v3(V.invInertia[b]);
     if (norm2(iIa) == 0.0f && norm2(iIb) == 0.0f) return;
@@ -156,16 +204,23 @@ __device__ __forceinline__ void projectBendAt(const RodView& V, int k, int a, in
 
     if (norm2(iIa) > 0.0f) {
         const V3 g = (dL * -p.w - cross(im(p), dL)) * (1.0f / lbar);
-        V.q[a] = f4(applyBodyDelta(qa, cwise(iIa, g)));
+        if (COMP)
+            rotateFrameComp(V, a, cwise(iIa, g) * 0.5f);
+        else
+            V.q[a] = f4(applyBodyDelta(qa, cwise(iIa, g)));
     }
     if (norm2(iIb) > 0.0f) {
         const V3 g = (dL * p.w - cross(im(p), dL)) * (1.0f / lbar);
-        V.q[b] = f4(applyBodyDelta(qb, cwise(iIb, g)));
+        if (COMP)
+            rotateFrameComp(V, b, cwise(iIb, g) * 0.5f);
+        else
+            V.q[b] = f4(applyBodyDelta(qb, cwise(iIb, g)));
     }
 }
 
+template <bool COMP>
 __device__ __forceinline__ void projectBendOne(const RodView& V, int k, float invH2) {
-    projectBendAt(V, k, V.bA[k], V.bB[k], invH2);
+    projectBendAt<COMP>(V, k, V.bA[k], V.bB[k], invH2);
 }
 
 // ---------------------------------------------------------------- world contacts
@@ -529,17 +584,23 @@ __device__ __forceinline__ void predictParticle(const RodView& V, int i, float h
     addPos<COMP>(V, i, vn * h);
 }
 
+template <bool COMP>
 __device__ __forceinline__ void predictFrame(const RodView& V, int j, float h) {
     const float4 qs = V.q[j];
-    V.qPrev[j] = qs;
+    // compensated: the substep's accumulated rotation starts at identity
+    V.qPrev[j] = COMP ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : qs;
     const V3 iI = v3(V.invInertia[j]);
     if (norm2(iI) == 0.0f) return;
+    if (COMP) renormalizeFrameComp(V, j);  // once per substep, in FP64
     const V3 w = v3(V.omega[j]);
-    const Q4 q = q4(qs);
+    const Q4 q = q4(V.q[j]);
     const V3 tau = rotateInv(q, v3(V.torque[j]));
     const V3 wn = w + cwise(iI, tau - cross(w, cwise(v3(V.inertia[j]), w))) * h;
     V.omega[j] = f4(wn);
-    V.q[j] = f4(qnormalize(qadd(q, qscale(qmul(q, qmake(0.0f, wn)), 0.5f * h))));
+    if (COMP)
+        rotateFrameComp(V, j, wn * (0.5f * h));
+    else
+        V.q[j] = f4(qnormalize(qadd(q, qscale(qmul(q, qmake(0.0f, wn)), 0.5f * h))));
 }
 
 template <bool COMP>
@@ -552,12 +613,19 @@ __device__ __forceinline__ void finishParticle(const RodView& V, int i, float h,
     V.v[i] = f4(divs(d, h) * linDecay);
 }
 
+template <bool COMP>
 __device__ __forceinline__ void finishFrame(const RodView& V, int j, float h, float angDecay) {
     if (norm2(v3(V.invInertia[j])) == 0.0f) {
         V.omega[j] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         return;
     }
-    const Q4 dq = sameHemisphereId(qmul(conj(q4(V.qPrev[j])), q4(V.q[j])));
+    Q4 dq;
+    if (COMP) {
+        const Q4 e = q4(V.qPrev[j]);  // the substep's rotation 1 + e
+        dq = sameHemisphereId(Q4{1.0f + e.w, e.x, e.y, e.z});
+    } else {
+        dq = sameHemisphereId(qmul(conj(q4(V.qPrev[j])), q4(V.q[j])));
+    }
     V.omega[j] = f4(im(dq) * (2.0f / h) * angDecay);
 }
 
