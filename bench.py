@@ -42,6 +42,10 @@ FLOPS_PER_SEG_SUBSTEP = {"grid": 890.5, "uneven": 880.5, "cantilever": 880.5}
 # (x, v, force, kinematic velocity per particle; q, omega, torque per frame;
 # float4 rows): read 4 x 16 + 3 x 16, written 2 x 16 + 2 x 16.
 BYTES_PER_SEG_STEP = 7 * 16 + 4 * 16
+# Measured DRAM bytes (read + write) per segment-step of the batched step,
+# from one ncu capture of a 4096-rod uneven batch (state beyond L2, so the
+# figure scales with segments: 265.9 MB over 1 084 256 segments).
+DRAM_BYTES_PER_SEG_STEP = {"uneven": 245.4}
 
 
 def measured_peaks():
@@ -416,7 +420,10 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "achieved": bytes_alg / per_launch_s / 1e9,
                      "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
                      "frac": bytes_alg / per_launch_s / 1e9 / peaks.get("hbm_gbs", 6650.0),
-                     "traffic": None, "note": "of measured; the step is FP32-pipe bound, see fp32"},
+                     "traffic": (DRAM_BYTES_PER_SEG_STEP[args.workload] * int(wl.segments.sum())
+                                 if args.workload in DRAM_BYTES_PER_SEG_STEP else None),
+                     "note": "of measured; traffic per launch from ncu on 4096 rods scaled by segments; "
+                             "the step is FP32-latency bound, see fp32"},
         "fp32": {"achieved": flops / per_launch_s / 1e12, "peak": fp32_peak, "unit": "TFLOP/s",
                  "frac": flops / per_launch_s / 1e12 / fp32_peak,
                  "flops_per_segment_substep": FLOPS_PER_SEG_SUBSTEP.get(args.workload, 880.5)},
