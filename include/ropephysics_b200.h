@@ -436,6 +436,25 @@ rp_status rp_server_get_stats(rp_server* server, rp_server_stats* out);
 /* Blocks until nothing is queued or running; RP_ERR_NOT_READY on timeout. */
 rp_status rp_server_drain(rp_server* server, double timeout_s);
 
+/* ---- trajectory files ----
+ * reference: the .rodtraj writer of the demo scenes (TrajectoryWriter,
+ * src/validation/scenes.cpp:13-20 format, :44-90 writer), fed here from the
+ * batch's device buffers without a synchronising download: each append packs
+ * the positions on the batch's stream (compensation applied), copies them and
+ * the contact states into pinned buffers and returns; a writer thread writes
+ * the frame while the next steps run (two frames in flight at most). A frame
+ * is the caller's seconds value, every rod's positions (rod-major) and the
+ * contact points: the particles of world-contact slots that pushed in the
+ * last step. Every rod must have the same particle count (the format's).
+ * Close the trajectory before destroying its batch. */
+typedef struct rp_traj rp_traj;
+rp_status rp_traj_open(const char* path, int32_t num_frames, const rp_batch* batch, float radius, float fps,
+                       rp_traj** out);
+rp_status rp_traj_append(rp_traj* traj, rp_batch* batch, float seconds);
+/* Waits for the queued frames, corrects the header's frame count if fewer or
+ * more than declared were appended, closes the file and frees the writer. */
+rp_status rp_traj_close(rp_traj* traj, int32_t* frames_written);
+
 #ifdef __cplusplus
 }
 #endif

@@ -25,7 +25,8 @@ from . import _abi
 
 __all__ = ["RopeError", "Strategy", "Precision", "ContactState", "Material", "Primitive", "World",
            "StepParams", "Drive", "Rod", "Batch", "Server", "cuda_available", "device_name",
-           "diagnostic", "max_fused_segments", "coloring", "self_collision_index_gap", "lib"]
+           "diagnostic", "max_fused_segments", "coloring", "self_collision_index_gap", "lib", "Trajectory",
+           "read_rodtraj"]
 
 
 def lib():
@@ -680,3 +681,59 @@ class Server:
 
     def drain(self, timeout: float = 600.0):
         _check(lib().rp_server_drain(self._h, float(timeout)))
+
+
+class Trajectory:
+    """A .rodtraj file written from a batch's device buffers (the reference's
+    demo-scene trajectory format, src/validation/scenes.cpp:13-20)."""
+
+    def __init__(self, path: str, num_frames: int, batch: "Batch", radius: float, fps: float):
+        h = C.c_void_p()
+        _check(lib().rp_traj_open(str(path).encode(), num_frames, batch._h, radius, fps, C.byref(h)))
+        self._h = h
+        self._batch = batch
+
+    def append(self, seconds: float = 0.0):
+        """Queue the batch's current positions and contacts as the next frame."""
+        _check(lib().rp_traj_append(self._h, self._batch._h, float(seconds)))
+
+    def close(self) -> int:
+        """Write the queued frames, close the file; returns the frame count."""
+        if not self._h:
+            return 0
+        n = C.c_int32()
+        h, self._h = self._h, None
+        _check(lib().rp_traj_close(h, C.byref(n)))
+        return n.value
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def read_rodtraj(path: str) -> dict:
+    """Parse a .rodtraj file: header fields and per-frame seconds, positions
+    (rods x particles x 3) and contact points (n x 3)."""
+    data = open(path, "rb").read()
+    if data[:8] != b"RODTRAJ1":
+        raise ValueError("not a RODTRAJ1 file")
+    frames, rods, particles = np.frombuffer(data, np.int32, 3, 8)
+    radius, fps = np.frombuffer(data, np.float32, 2, 20)
+    at = 28
+    out = {"num_frames": int(frames), "num_rods": int(rods), "num_particles": int(particles),
+           "radius": float(radius), "fps": float(fps), "seconds": [], "positions": [], "contacts": []}
+    for _ in range(int(frames)):
+        out["seconds"].append(float(np.frombuffer(data, np.float32, 1, at)[0]))
+        at += 4
+        n = int(rods) * int(particles) * 3
+        out["positions"].append(np.frombuffer(data, np.float32, n, at).reshape(int(rods), int(particles), 3))
+        at += 4 * n
+        nc = int(np.frombuffer(data, np.int32, 1, at)[0])
+        at += 4
+        out["contacts"].append(np.frombuffer(data, np.float32, 3 * nc, at).reshape(nc, 3))
+        at += 12 * nc
+    if at != len(data):
+        raise ValueError(f"{len(data) - at} trailing bytes")
+    return out

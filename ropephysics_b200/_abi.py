@@ -154,6 +154,9 @@ SIGNATURES = {
     "rp_server_release": (i32, [vp, C.c_uint64]),
     "rp_server_get_stats": (i32, [vp, P(ServerStats)]),
     "rp_server_drain": (i32, [vp, f64]),
+    "rp_traj_open": (i32, [C.c_char_p, i32, vp, f32, f32, pp]),
+    "rp_traj_append": (i32, [vp, vp, f32]),
+    "rp_traj_close": (i32, [vp, P(i32)]),
 }
 
 _lib = None

@@ -569,6 +569,24 @@ rp_status syncBatch(rp_batch* b) {
 
 // ---------------------------------------------------------------- C ABI
 
+namespace rpx {
+BatchView batchView(const rp_batch* b) {
+    BatchView v;
+    v.device = b->device;
+    v.stream = b->stream;
+    v.x = b->a.x;
+    v.xComp = b->a.xComp;
+    v.contactState = b->a.contactState;
+    v.compensated = (b->precision & RP_PRECISION_COMPENSATED) != 0;
+    v.totalP = b->totalP;
+    v.totalSlots = b->totalSlots;
+    v.rods = b->rods.data();
+    v.particlesOfRod = b->tmplNP.data();
+    v.numRods = b->numRods;
+    return v;
+}
+}  // namespace rpx
+
 extern "C" {
 
 int32_t rp_abi_version(void) { return RP_ABI_VERSION; }

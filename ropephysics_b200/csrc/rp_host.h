@@ -56,4 +56,19 @@ size_t planGroups(const std::vector<int32_t>& rodIds, const rp::DRod* rods, cons
                   int cta, int pairsPerThread, bool comp, std::vector<int32_t>& order,
                   std::vector<int32_t>& groups);
 
+// ---- rp_batch.cpp: what the trajectory writer reads of a batch ----
+struct BatchView {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    const float4* x = nullptr;
+    const float4* xComp = nullptr;
+    const uint8_t* contactState = nullptr;
+    bool compensated = false;
+    int64_t totalP = 0, totalSlots = 0;
+    const rp::DRod* rods = nullptr;  // host copies, numRods entries
+    const int* particlesOfRod = nullptr;
+    int numRods = 0;
+};
+BatchView batchView(const rp_batch* b);
+
 }  // namespace rpx

@@ -32,6 +32,9 @@ cudaError_t batchedOccupancy(int threads, size_t smemBytes, int* blocksPerSm);
 // first call per device, with that device current).
 cudaError_t staticScratch(void** ptr, size_t* bytes);
 
+// xyz of n particles packed as 3 floats each (compensated: x - xComp).
+cudaError_t launchPackPositions(const float4* x, const float4* xComp, float* out, int64_t n, cudaStream_t stream);
+
 // One hold observation of every armed rod (the final sample of a run).
 cudaError_t launchObserve(const DArgs& a, int compensated, cudaStream_t stream);
 

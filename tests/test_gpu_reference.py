@@ -43,7 +43,8 @@ def test_self_pairs_bit_exact_vs_reference_gpu(reference_gpu, oracle64):
     """Self-contact pair lists -- membership and order -- equal the reference
     FP32 GPU kernel's from identical input state: the coiled rope restart of
     gpu_cases.cpp:437-484 and tightly coiled rods with dozens of contacts,
-    at several hash-table sizes."""
+    at several hash-table sizes, including coils dense enough to overflow the
+    pool (equal truncation and equal overflow counts)."""
     R = reference_gpu
     if not R.lib.refgpu_available():
         pytest.skip("no device for the reference GPU path")
@@ -61,8 +62,17 @@ def test_self_pairs_bit_exact_vs_reference_gpu(reference_gpu, oracle64):
         o.bRestD[:] = 0.0
         cases.append((o, OW([OP.plane((0, 0, pts[:, 2].min() - 0.004), (0, 0, 1), 0.6)],
                             self_collision=True, self_friction=0.4, hash_table_size=table)))
+    # denser coils: adjacent turns pressed together, so the contacts exceed
+    # the pool's capacity max(16, nSt / 2) and both paths must truncate alike
+    for table in (128, 512):
+        n = int(rng.integers(120, 220))
+        pts = W.helix(n, 0.2 * n / 32, float(rng.uniform(0.02, 0.03)), pitch=1.6 * 5e-3)
+        o = oracle64.centerline(pts, youngs=1e8, poisson=0.3, density=1100.0, radius=5e-3)
+        o.bRestD[:] = 0.0
+        cases.append((o, OW([], self_collision=True, self_friction=0.4, hash_table_size=table)))
     from tests.helpers import product_rod
     total = 0
+    overflowed = 0
     for orod, ow in cases:
         h = _ref_from(R, orod)
         wh = R.world(ow)
@@ -73,6 +83,8 @@ def test_self_pairs_bit_exact_vs_reference_gpu(reference_gpu, oracle64):
         R.lib.refgpu_step(rb, one.dt, 1, one.iterations, g, 0.0, 0.0, 1, 1)
         R.lib.refgpu_sync(rb)
         expect = R.gpu_self_pairs(rb)
+        ref_overflow = int(R.lib.refgpu_overflow(rb))
+        overflowed += ref_overflow > 0
         pw = rp.World([rp.Primitive(p.type, p.a, p.b, p.normal, p.half_extents, p.rotation,
                                     p.radius, p.friction) for p in ow.primitives],
                       self_collision=True, self_friction=ow.self_friction,
@@ -83,11 +95,13 @@ def test_self_pairs_bit_exact_vs_reference_gpu(reference_gpu, oracle64):
             b.step(one)
             got = [tuple(int(v) for v in p) for p in b.read_self_contacts(0)]
             assert got == expect, (s, ow.hash_table_size, len(got), len(expect))
+            assert b.self_contact_overflow() == ref_overflow, (s, ref_overflow)
             b.close()
         total += len(expect)
         R.lib.refgpu_free(rb)
         R.free(h)
     assert total >= 40
+    assert overflowed >= 1  # the truncation path was exercised
 
 
 def test_contact_active_sets_vs_reference_gpu(reference_gpu, oracle64):
