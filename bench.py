@@ -37,7 +37,7 @@ sys.path.insert(0, ROOT)
 # mul, div, sqrt), counted exactly by the op-counting oracle build
 # (liboracle_count.so; tests/test_oracle.py pins these values). Contacts add
 # ~10 per (particle, primitive) slot.
-FLOPS_PER_SEG_SUBSTEP = {"grid": 890.5, "uneven": 880.5, "cantilever": 880.5}
+FLOPS_PER_SEG_SUBSTEP = {"grid": 890.5, "uneven": 880.5, "cantilever": 880.5, "hook": 890.5}
 # Algorithmic HBM bytes per segment per step: state read once and written once
 # (x, v, force, kinematic velocity per particle; q, omega, torque per frame;
 # float4 rows): read 4 x 16 + 3 x 16, written 2 x 16 + 2 x 16.
@@ -301,6 +301,49 @@ def run_served(capacity: float, seconds: float, seed: int, load: float, budget_g
 # ----------------------------------------------------------------------------- GPU arm
 
 
+def measure_shapes(stream, fp32_peak: float) -> dict:
+    """The other named shapes, batched and plain, short timed runs on the same
+    GPU: the clamped 64-segment cantilever with a tip load (latency of one
+    rod), the 4096 x 64 driven grid over a floor, and the 3600-cable hook
+    sweep in mixed precision (compensated positions and frames, FP64 cone and
+    verdicts). Device time with CUDA events after 3 warm-up steps."""
+    import torch
+
+    import ropephysics_b200 as rp
+    from ropephysics_b200 import workloads as W
+
+    mixed = rp.Precision.COMPENSATED | rp.Precision.FP64_CONE | rp.Precision.FP64_VERDICT
+    out = {}
+    for key, wl, prec, steps in (("cantilever", W.cantilever(), rp.Precision.REFERENCE, 200),
+                                 ("grid", W.grid(4096), rp.Precision.REFERENCE, 20),
+                                 ("hook", W.hook(), mixed, 20)):
+        seg_sub = wl.segment_substeps_per_step()
+        rates = {}
+        for label, strat in (("batched", rp.Strategy.BATCHED), ("plain", rp.Strategy.FUSED)):
+            b = wl.make_batch(strat)
+            b.set_precision(int(prec))
+            b.set_stream(stream.cuda_stream)
+            b.set_graph(True)
+            b.step_many(wl.params, 3)
+            b.step_many(wl.params, steps)
+            b.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            b.step_many(wl.params, steps)
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            rates[label] = (seg_sub / (ms / 1e3), ms)
+            b.close()
+        flops = FLOPS_PER_SEG_SUBSTEP.get(key, 890.5)
+        out[key] = {"workload": wl.name, "precision": int(prec), "unit": "segment-substeps/s",
+                    "batched": rates["batched"][0], "plain": rates["plain"][0],
+                    "speedup": rates["batched"][0] / rates["plain"][0],
+                    "ms_per_step_batched": rates["batched"][1], "ms_per_step_plain": rates["plain"][1],
+                    "fp32_frac_batched": rates["batched"][0] * flops / 1e12 / fp32_peak}
+    return out
+
+
 def run_ours(args):
     world_size, rank, local = dist_setup(args)
     import torch
@@ -429,6 +472,8 @@ def run_ours(args):
                  "flops_per_segment_substep": FLOPS_PER_SEG_SUBSTEP.get(args.workload, 880.5)},
         "clocks": clk,
     }
+    if not args.no_shapes:
+        line["shapes"] = measure_shapes(stream, fp32_peak)
     if not args.no_served:
         batch.close()
         line["served"] = run_served(value / world_size, args.served_seconds, args.seed + 7 + rank,
@@ -488,6 +533,7 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--no-shapes", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-rods", type=int, default=64)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)

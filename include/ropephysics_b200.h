@@ -65,7 +65,9 @@ typedef enum rp_strategy {
 
 /* Precision flags (bitwise OR). 0 = reference order: every FP32 operation in
  * the order of the reference kernel, for parity with its GPU path.
- *   RP_PRECISION_COMPENSATED  Kahan-compensated position accumulation.
+ *   RP_PRECISION_COMPENSATED  Kahan-compensated positions and frames (frames
+ *                             renormalised in FP64 once per substep; uploads
+ *                             keep the double inputs' rounding residuals).
  *   RP_PRECISION_FP64_CONE    the Coulomb stick/slip cap test in FP64.
  *   RP_PRECISION_FP64_VERDICT near-boundary hold/slide classification in FP64. */
 typedef enum rp_precision {
@@ -141,7 +143,9 @@ typedef struct rp_primitive {
     double friction;
 } rp_primitive;
 
-/* Collision world (reference: CollisionWorld, collision.h:83-106). */
+/* Collision world (reference: CollisionWorld, collision.h:83-106). At most 64
+ * primitives per world (the batched kernel culls them per rod with a 64-bit
+ * mask); the reference has no limit. */
 typedef struct rp_world {
     const rp_primitive* primitives;
     int32_t num_primitives;

@@ -163,3 +163,17 @@ def test_no_device_is_an_error_not_a_fallback():
     assert e.value.status == 2
     assert "no usable CUDA device" in rp.diagnostic()
     assert rp.max_fused_segments() == 0
+
+
+def test_world_limits_rejected_before_any_device_work():
+    """At most 64 primitives per world (the batched kernel culls them with a
+    64-bit mask); self-collision needs a hash table of 1..2^20 buckets."""
+    import ropephysics_b200 as rp
+    rod = rp.Rod.straight(8, 0.2, rp.Material())
+    many = [rp.Primitive.sphere((0, 0, -1.0 - k), 0.1, 0.5) for k in range(65)]
+    with pytest.raises(rp.RopeError) as e:
+        rp.Batch.create(rod, 1, rp.Strategy.BATCHED, rp.World(many))
+    assert e.value.status == 1 and "64" in str(e.value)
+    with pytest.raises(rp.RopeError) as e:
+        rp.Batch.create(rod, 1, rp.Strategy.BATCHED, rp.World([], self_collision=True, hash_table_size=0))
+    assert e.value.status == 1
