@@ -355,7 +355,7 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
                     *touching = 0;
                 }
             }
-            if (V.numPrims > 0) {
+            if (V.numPrims > 0 && maskNow != 0ull) {  // team-uniform; a fully culled world has no slot
                 for (int i = lane; i < nP; i += team) generateSlotsMasked(V, i, regenerate, maskNow);
             }
             if (self) {
@@ -507,8 +507,8 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
                         teamSync(team, teamIdx);
                     }
                 }
-                if (V.numPrims > 0) {
-                    for (int i = lane; i < nP; i += team) projectSlots<COMP, FP64>(V, i, *primMask);
+                if (V.numPrims > 0 && maskNow != 0ull) {
+                    for (int i = lane; i < nP; i += team) projectSlots<COMP, FP64>(V, i, maskNow);
                     teamSync(team, teamIdx);
                 }
                 if (self) {
