@@ -254,8 +254,8 @@ rp_status rp_batch_step(rp_batch* batch, const rp_step_params* params);
 rp_status rp_batch_step_many(rp_batch* batch, const rp_step_params* params, int32_t steps);
 /* No reference counterpart. One step of an RP_STRATEGY_BATCHED batch, the
  * same kernel and the same results as rp_batch_step, but the step's scratch
- * (work-queue counters, start-of-substep frames, world-contact slots,
- * self-contact pool) is carved from a fixed static device array of
+ * (work-queue counters, start-of-substep frames under compensated
+ * precision, world-contact slots, self-contact pool) is carved from a fixed static device array of
  * RP_STATIC_SCRATCH_BYTES instead of the batch's own buffers, and the call
  * allocates no device memory. Needs: 256 + 16 x frames + 32 x contact slots
  * (+ 64 x self-contact pool entries), each section rounded up to 256 bytes;

@@ -207,7 +207,7 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
     const RodLayout L = rodLayout(nP, nS, nSt, nB, R.numPrims, R.selfCollision, R.hashTableSize,
                                   R.selfCapacity, 1, COMP ? 1 : 0);
     V.q = reinterpret_cast<float4*>(base + L.q);
-    V.qPrev = A.gqPrev + R.sOff;
+    V.qPrev = COMP ? A.gqPrev + R.sOff : reinterpret_cast<float4*>(base + L.qPrev);
     V.x = reinterpret_cast<float4*>(base + L.x);
     V.xPrev = reinterpret_cast<float4*>(base + L.xPrev);
     V.xComp = COMP ? reinterpret_cast<float4*>(base + L.xComp) : A.xComp + R.pOff;

@@ -4,13 +4,14 @@
 // Per rod, in bytes (16-byte aligned sections). The full layout (plain
 // kernel) stages every state array, as the reference's fused kernel does. The
 // lean layout (batched kernel) keeps what every substep reads and writes --
-// positions and their start-of-substep copies, frames, velocities, angular
-// velocities, multipliers, the hash -- and leaves in global memory what a
-// step only reads (loads, kinematic velocities), what is touched once per
-// substep (qPrev) or only when a contact is live (world contact slots of
-// primitives that survive the per-rod cull, the self-contact pool); those
-// stay L1/L2-resident.
-//   frames     q [, qPrev], omega [, torque]         16 x nS each
+// positions and their start-of-substep copies, frames and (except under
+// compensation, where the shared memory is worth more as occupancy) their
+// start-of-substep copies, velocities, angular velocities, multipliers, the
+// hash -- and leaves in global memory what a step only reads (loads,
+// kinematic velocities) or touches only when a contact is live (world
+// contact slots of primitives that survive the per-rod cull, the
+// self-contact pool); those stay L1/L2-resident.
+//   frames     q, qPrev (not lean+comp), omega [, torque]  16 x nS each
 //   particles  x, xPrev, v [, force, kin], xComp     16 x nP each (xComp: full,
 //                                                    or lean with compensation)
 //   frames     qComp                                 16 x nS (lean with compensation)
@@ -56,7 +57,7 @@ RP_HD inline RodLayout rodLayout(int32_t nP, int32_t nS, int32_t nSt, int32_t nB
     RodLayout L;
     int32_t o = 0;
     L.q = o;      o += 16 * nS;
-    if (!lean) {
+    if (!lean || !comp) {  // lean + compensated: in global memory, to keep occupancy
         L.qPrev = o;  o += 16 * nS;
     } else {
         L.qPrev = -1;

@@ -129,3 +129,28 @@ def test_oversized_request_rejected():
         server.submit([rod] * 64, 10)
     assert e.value.status == 6
     server.close()
+
+
+def test_concurrent_submitters():
+    """Four host threads submit at once; every result still equals its request
+    run alone (the submit path is thread-safe; ctypes releases the GIL)."""
+    import threading
+    reqs = small_requests(9, 12)
+    alone = [run_alone(r) for r in reqs]
+    server = rp.Server(512 << 20, PARAMS)
+    ids = [None] * len(reqs)
+
+    def worker(k):
+        for i in range(k, len(reqs), 4):
+            ids[i] = submit(server, reqs[i])
+
+    threads = [threading.Thread(target=worker, args=(k,)) for k in range(4)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert len(set(ids)) == len(reqs)
+    for rid, x in zip(ids, alone):
+        server.wait(rid, 300)
+        assert np.array_equal(server.result(rid), x)
+    server.close()
