@@ -10,10 +10,11 @@ steps (50 ms) and at the end; held <=> max rise <= 0.05 m.
 
 The 200 placements nearest the capstan boundary mu = ln(ratio) / pi are
 re-run on the reference's own FP64 CPU solver (compiled from its sources,
-colour-ordered, observed by its own HangOutcome). These are the placements
-where single precision is known to flip verdicts; the agreement is asserted
-and printed for both this library's mixed-precision mode and its
-reference-order FP32 mode.
+colour-ordered, observed by its own HangOutcome) and on its own FP32 GPU
+batch (run as its harness runs a sweep). These are the placements where
+single precision is known to flip verdicts; the mixed-precision mode's
+agreement with FP64 is asserted (>= 180 of 200, and no less than the
+reference GPU kernel's), and printed for the reference-order FP32 mode too.
 """
 import math
 import os
@@ -40,6 +41,55 @@ def gpu_verdicts(wl, precision):
     assert b.error_count() == 0
     b.close()
     return rise, held, near
+
+
+def reference_gpu_verdicts(ratios, mus, youngs, p):
+    """Hold/slide of the given placements on the reference's own GPU batch,
+    run the way its harness runs a sweep (heldOnGpu,
+    src/validation/application_cases.cpp:38-70): one fused batch per
+    (friction, stiffness) -- the batch shares one world and one prototype --
+    every ratio uploaded as a rod, HangOutcome from the rod's double start
+    height and the downloaded FP32 positions every INTERVAL steps and at the
+    end. None without the reference GPU build."""
+    try:
+        from oracle import Reference
+        R = Reference(gpu=True)
+    except Exception:
+        return None
+    if not R.lib.refgpu_available():
+        return None
+    import ctypes as C
+    held = np.zeros(len(ratios), np.uint8)
+    g = (C.c_double * 3)(*p.gravity)
+    fp = C.POINTER(C.c_float)
+    groups = {}
+    for n, key in enumerate(zip(mus, youngs)):
+        groups.setdefault(key, []).append(n)
+    for (mu, E), members in groups.items():
+        handles = [R.hanging(float(ratios[n]), float(E), length=1.2, segments=120, bar_radius=0.02,
+                             bar_height=0.8) for n in members]
+        wh = R.world(OW([OP.capsule((0, -0.3, 0.8), (0, 0.3, 0.8), 0.02, float(mu)),
+                         OP.plane((0, 0, 0), (0, 0, 1), float(mu))],
+                        self_collision=True, self_friction=float(mu), hash_table_size=256))
+        rb = R.lib.refgpu_create(handles[0], len(members), 1, wh)
+        assert rb
+        z0 = []
+        for r, h in enumerate(handles):
+            R.lib.refgpu_upload_rod(rb, r, h)
+            z0.append(float(R.export(h).x[0][2]))
+        pos = np.zeros((len(members), 121, 3), np.float32)
+        rise = np.zeros(len(members))
+        for s in range(1, STEPS + 1):
+            R.lib.refgpu_step(rb, p.dt, p.substeps, p.iterations, g, 0.0, 0.0, 1, 1)
+            if s % INTERVAL == 0 or s == STEPS:
+                R.lib.refgpu_download_positions(rb, pos.ctypes.data_as(fp))
+                rise = np.maximum(rise, pos[:, 0, 2].astype(np.float64) - np.array(z0))
+        for r, n in enumerate(members):
+            held[n] = 1 if rise[r] <= 0.05 else 0
+        R.lib.refgpu_free(rb)
+        for h in handles:
+            R.free(h)
+    return held
 
 
 def test_hook_sweep_verdicts_vs_fp64_cpu(reference):
@@ -73,11 +123,15 @@ def test_hook_sweep_verdicts_vs_fp64_cpu(reference):
     rise_c, held_c = reference.hold_many(handles, worlds, p, STEPS, INTERVAL, os.cpu_count() or 1)
     for h in handles:
         reference.free(h)
+    held_g = reference_gpu_verdicts(ratios[r_i[nearest]], mus[m_i[nearest]], [Es[e] for e in e_i[nearest]], p)
     agree_m = int(np.sum(held_m[nearest] == held_c))
     agree_f = int(np.sum(held_f[nearest] == held_c))
+    agree_g = int(np.sum(held_g == held_c)) if held_g is not None else None
     print(f"\nhook sweep: held {held_m.sum()}/3600 (mixed) {held_f.sum()}/3600 (FP32); "
           f"200 nearest the capstan boundary: mixed agrees {agree_m}/200, FP32 {agree_f}/200, "
-          f"near-boundary flags {int(near_m[nearest].sum())}")
+          f"reference GPU kernel (FP32) {agree_g}/200, near-boundary flags {int(near_m[nearest].sum())}")
     assert agree_m >= 180
+    if agree_g is not None:  # the mixed mode agrees with FP64 at least as often as the reference kernel
+        assert agree_m >= agree_g
     # the sweep is not degenerate: both outcomes occur
     assert 0 < held_m.sum() < 3600
