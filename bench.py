@@ -285,10 +285,15 @@ def run_served(capacity: float, seconds: float, seed: int, load: float, budget_g
     work = sum(i["segment_substeps"] for i in done)
     span = (max(i["done_s"] for i in done) - min(i["submit_s"] for i in infos)) if done else 0.0
     server.close()
-    pct = lambda p: float(np.percentile(lat, p)) if lat else None
+    pct = lambda v, p: float(np.percentile(v, p)) if v else None
+    wait = sorted(i["admit_s"] - i["submit_s"] for i in done)  # queued behind the budget
+    steps_per_s = [i["segment_substeps"] / max(i["done_s"] - i["admit_s"], 1e-9) for i in done]
     return {
         "requests": len(ids), "completed": len(done), "drained": drained, "rejected": len(errors),
-        "p50_latency_s": pct(50), "p99_latency_s": pct(99), "mean_latency_s": float(np.mean(lat)) if lat else None,
+        "p50_latency_s": pct(lat, 50), "p99_latency_s": pct(lat, 99),
+        "mean_latency_s": float(np.mean(lat)) if lat else None,
+        "p50_queue_wait_s": pct(wait, 50), "p99_queue_wait_s": pct(wait, 99),
+        "p50_request_rate": pct(steps_per_s, 50),
         "sustained": work / span if span > 0 else None, "unit": "segment-substeps/s",
         "busy_s": st["busy_s"], "arrival_rate_req_s": rate, "window_s": seconds,
         "load_vs_capacity": load, "spec_rate_req_s": spec_rate,
