@@ -128,12 +128,11 @@ __device__ __forceinline__ int bucketMultiplicity(float4 cj, float4 ck, float ce
 // by its block maximum (float max, add and multiply are monotone), so every
 // pair the sphere test keeps is reached.
 __device__ void countSelfByBlocks(const RodView& V, const SelfScratch& S, int nSt, int gap, int table,
-                                  int lane, int team, int32_t* touching) {
+                                  float cell, int lane, int team, int32_t* touching) {
     if (nSt <= gap) return;
     const int wl = lane & 31, warp = lane >> 5, warps = team >> 5;
     const int nBlk = (nSt + 7) >> 3;
     const float twoR = 2.0f * V.radius;
-    const float cell = *S.cellSize;
     for (int J = warp; J < nBlk; J += warps) {
         const float4 jlo = S.blocks[2 * J], jhi = S.blocks[2 * J + 1];
         const int jmin = 8 * J;
@@ -306,13 +305,40 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
                 float lx = 3.0e38f, ly = 3.0e38f, lz = 3.0e38f;
                 float hx = -3.0e38f, hy = -3.0e38f, hz = -3.0e38f;
                 if (self) {
-                    for (int j = lane; j < nSt; j += team) {
-                        const int p0 = T.chain ? j : V.sP0[j], p1 = T.chain ? j + 1 : V.sP1[j];
-                        const V3 a = v3(V.x[p0]), b = v3(V.x[p1]);
-                        const float len = norm(b - a);
-                        const V3 c = (a + b) * 0.5f;
-                        S.centres[j] = make_float4(c.x, c.y, c.z, 0.5f * len);
-                        mx = fmaxf(mx, len);
+                    // whole warps per round (team is a multiple of 32), so the
+                    // 8-lane shuffles bounding each chain block of 8 segments
+                    // always have every lane present; the counts are zeroed
+                    // here too, so the count needs no barrier of its own
+                    for (int j0 = 0; j0 < nSt; j0 += team) {
+                        const int j = j0 + lane;
+                        float4 blo = make_float4(3.0e38f, 3.0e38f, 3.0e38f, 0.0f);
+                        float4 bhi = make_float4(-3.0e38f, -3.0e38f, -3.0e38f, 0.0f);
+                        if (j < nSt) {
+                            const int p0 = T.chain ? j : V.sP0[j], p1 = T.chain ? j + 1 : V.sP1[j];
+                            const V3 a = v3(V.x[p0]), b = v3(V.x[p1]);
+                            const float len = norm(b - a);
+                            const V3 c = (a + b) * 0.5f;
+                            S.centres[j] = make_float4(c.x, c.y, c.z, 0.5f * len);
+                            S.segCount[j] = 0;
+                            mx = fmaxf(mx, len);
+                            blo = make_float4(c.x, c.y, c.z, 0.5f * len);
+                            bhi = make_float4(c.x, c.y, c.z, 1.0f + fabsf(c.x) + fabsf(c.y) + fabsf(c.z));
+                        }
+#pragma unroll
+                        for (int o = 1; o < 8; o <<= 1) {
+                            blo.x = fminf(blo.x, __shfl_xor_sync(0xffffffffu, blo.x, o));
+                            blo.y = fminf(blo.y, __shfl_xor_sync(0xffffffffu, blo.y, o));
+                            blo.z = fminf(blo.z, __shfl_xor_sync(0xffffffffu, blo.z, o));
+                            blo.w = fmaxf(blo.w, __shfl_xor_sync(0xffffffffu, blo.w, o));
+                            bhi.x = fmaxf(bhi.x, __shfl_xor_sync(0xffffffffu, bhi.x, o));
+                            bhi.y = fmaxf(bhi.y, __shfl_xor_sync(0xffffffffu, bhi.y, o));
+                            bhi.z = fmaxf(bhi.z, __shfl_xor_sync(0xffffffffu, bhi.z, o));
+                            bhi.w = fmaxf(bhi.w, __shfl_xor_sync(0xffffffffu, bhi.w, o));
+                        }
+                        if ((lane & 7) == 0 && j < nSt) {
+                            S.blocks[2 * (j >> 3)] = blo;
+                            S.blocks[2 * (j >> 3) + 1] = bhi;
+                        }
                     }
                 }
                 if (V.numPrims > 0) {
@@ -334,7 +360,9 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
                     row[0] = mx; row[1] = lx; row[2] = ly; row[3] = lz;
                     row[4] = hx; row[5] = hy; row[6] = hz;
                 }
-                teamSync(team, teamIdx);  // centres and per-warp rows visible
+                // reset before the barrier: the count below follows without one
+                if (lane == 0) *touching = 0;
+                teamSync(team, teamIdx);  // centres, blocks, zeroed counts, rows visible
                 // every lane reduces the rows in the same order (max and min
                 // are exact), so every lane holds the same mask and cell size;
                 // lane 0 also publishes them for the later phases
@@ -351,8 +379,7 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
                 cellNow = mx + 2.0f * V.radius;
                 if (self && lane == 0) {
                     if (sub == 0) *S.overflow = 0;
-                    *S.cellSize = cellNow;
-                    *touching = 0;
+                    *S.cellSize = cellNow;  // for the fill pass, after later barriers
                 }
             }
             if (V.numPrims > 0 && maskNow != 0ull) {  // team-uniform; a fully culled world has no slot
@@ -362,24 +389,8 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
                 if (regenerate) {
                     const float cell = cellNow;
                     // ---- count: contacts per segment, by chain blocks ----
-                    const int nBlk = (nSt + 7) >> 3;
-                    for (int b = lane; b < nBlk; b += team) {
-                        float4 lo = make_float4(3.0e38f, 3.0e38f, 3.0e38f, 0.0f);
-                        float4 hi = make_float4(-3.0e38f, -3.0e38f, -3.0e38f, 0.0f);
-                        const int j1 = min(8 * b + 8, nSt);
-                        for (int j = 8 * b; j < j1; ++j) {
-                            const float4 c = S.centres[j];
-                            lo.x = fminf(lo.x, c.x); lo.y = fminf(lo.y, c.y); lo.z = fminf(lo.z, c.z);
-                            hi.x = fmaxf(hi.x, c.x); hi.y = fmaxf(hi.y, c.y); hi.z = fmaxf(hi.z, c.z);
-                            lo.w = fmaxf(lo.w, c.w);
-                            hi.w = fmaxf(hi.w, 1.0f + fabsf(c.x) + fabsf(c.y) + fabsf(c.z));
-                        }
-                        S.blocks[2 * b] = lo;
-                        S.blocks[2 * b + 1] = hi;
-                    }
-                    for (int j = lane; j < nSt; j += team) S.segCount[j] = 0;
-                    teamSync(team, teamIdx);
-                    countSelfByBlocks(V, S, nSt, R.selfGap, table, lane, team, touching);
+                    // chain-block bounds and zeroed counts come from the centre pass
+                    countSelfByBlocks(V, S, nSt, R.selfGap, table, cell, lane, team, touching);
                     teamSync(team, teamIdx);
                     int total = 0;
                     if (*touching) {  // team-uniform: one shared word read after the barrier
