@@ -469,7 +469,11 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
                         S.pool[c].applied = 0.0f;
                     }
                 }
-                teamSync(team, teamIdx);
+                // no barrier here: every read of positions above finished before
+                // an earlier barrier, the prediction below touches neither the
+                // pool nor the level tables, and what lane 0 writes last (live
+                // count, levels) is read only after the prediction's barrier --
+                // so the team predicts while lane 0 builds the levels
             }
             // the previous substep's velocity update runs here, fused with this
             // substep's prediction: nothing between them reads v or omega,
