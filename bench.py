@@ -346,7 +346,52 @@ def measure_shapes(stream, fp32_peak: float) -> dict:
                     "speedup": rates["batched"][0] / rates["plain"][0],
                     "ms_per_step_batched": rates["batched"][1], "ms_per_step_plain": rates["plain"][1],
                     "fp32_frac_batched": rates["batched"][0] * flops / 1e12 / fp32_peak}
+    out["harness"] = measure_harness(stream)
     return out
+
+
+def measure_harness(stream, attempts: int = 1024, steps: int = 630) -> dict:
+    """One learning iteration's attempt batch of the harness-routing task:
+    1024 motions on random cables (120 segments, 4 substeps x 4 sweeps, five
+    primitives), each gripper an on-device waypoint schedule. A tenth of the
+    6300-step schedule is timed, batched (autotuned) and plain, with CUDA
+    events; `s_per_iteration` scales it to the whole schedule."""
+    import numpy as np
+    import torch
+
+    import ropephysics_b200 as rp
+    from ropephysics_b200 import harness as H
+
+    t = H.HarnessTask()
+    rng = np.random.default_rng(0)
+    pols = [t.to_policy(t.hand_written_policy().reshape(-1) + 0.08 * rng.standard_normal(10))
+            for _ in range(attempts)]
+    youngs, friction = H.random_cables(rng, attempts)
+    p = t.params()
+    res = {"workload": f"harness-{attempts}x{t.segments}", "unit": "segment-substeps/s"}
+    seg_sub = attempts * t.segments * p.substeps
+    for label, strat in (("batched", rp.Strategy.BATCHED), ("plain", rp.Strategy.FUSED)):
+        b = rp.Batch.create(t.build(), attempts, strat, t.world())
+        b.set_stream(stream.cuda_stream)
+        b.set_material_scales(youngs, friction)
+        if strat == rp.Strategy.BATCHED:
+            b.autotune(p, max_steps_per_launch=4)
+        b.set_waypoint_drives([t.drive(q) for q in pols])
+        b.set_graph(True)
+        b.step_many(p, 20)
+        b.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        b.step_many(p, steps)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        res[label] = seg_sub / (ms / 1e3)
+        res[f"ms_per_step_{label}"] = ms
+        res[f"s_per_iteration_{label}"] = ms * t.steps() / 1e3
+        b.close()
+    res["speedup"] = res["batched"] / res["plain"]
+    return res
 
 
 def run_ours(args):

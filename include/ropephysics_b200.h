@@ -180,6 +180,61 @@ typedef struct rp_drive {
     float phase;     /* [rad] */
 } rp_drive;
 
+/* On-device waypoint schedule of one rod's pinned particle: a robot gripper
+ * following a motion (reference: HarnessTask::gripperAt and gripperVelocity,
+ * src/apps/harness_routing.h:56-83, harness_routing.cpp:81-106). From
+ * `start`, the particle passes through waypoints[0 .. count-1], taking
+ * legs[k] seconds to reach waypoint k with a smoothstep u^2 (3 - 2u) within
+ * the leg, then holds at the last one; its height stays `height`. A
+ * controller holds each velocity for steps_per_control steps: during step s
+ * (counted from when the drives are set) the kinematic velocity is
+ * (P((tick + 1) T) - P(tick T)) x (1 / T) with tick = s / steps_per_control
+ * and T = dt x steps_per_control, computed on the device in double with the
+ * same operations and roundings as the reference's host code and stored as
+ * floats -- the velocities the reference uploads once per control tick
+ * (application_cases.cpp:236-248), with no upload. particle < 0 disables the
+ * schedule for the rod. */
+#define RP_MAX_WAYPOINTS 8
+typedef struct rp_waypoint_drive {
+    int32_t particle;
+    int32_t count;             /* 1 .. RP_MAX_WAYPOINTS */
+    int32_t steps_per_control; /* >= 1 */
+    int32_t reserved;
+    double dt;                 /* the step the schedule is sampled with [s] */
+    double start[2];           /* x, y [m] */
+    double height;             /* z [m] */
+    double legs[RP_MAX_WAYPOINTS];         /* [s], > 0 */
+    double waypoints[RP_MAX_WAYPOINTS][2]; /* x, y [m] */
+} rp_waypoint_drive;
+
+/* A routing board (reference: HarnessTask, harness_routing.h:29-41): the
+ * cable must pass below peg A, above peg B, laid against each (within
+ * peg_radius + cable_radius + lay_slack of its centre line), and through the
+ * clip between its posts, down on the board (below clip_height). */
+typedef struct rp_harness_board {
+    double peg_a[2];
+    double peg_b[2];
+    double clip[2];
+    double peg_radius;
+    double clip_half_gap;
+    double clip_height;
+    double cable_radius;
+    double lay_slack;
+} rp_harness_board;
+
+/* reference: HarnessTask::Outcome, harness_routing.h:85-94 */
+typedef struct rp_harness_outcome {
+    double score;     /* 3 on success; smooth for learning */
+    double side_a;    /* signed offset of the crossing nearest peg A [m] */
+    double side_b;
+    double clip_miss; /* distance from the clip centre line [m] */
+    uint8_t below_a;
+    uint8_t above_b;
+    uint8_t through_clip;
+    uint8_t success;
+    uint8_t reserved[4];
+} rp_harness_outcome;
+
 typedef struct rp_rod rp_rod;     /* host-side rod descriptor owned by the library */
 typedef struct rp_batch rp_batch; /* device-resident batch */
 
@@ -314,6 +369,17 @@ rp_status rp_batch_set_material_scales(rp_batch* batch, const float* youngs_scal
 rp_status rp_batch_set_drives(rp_batch* batch, const rp_drive* drives, int32_t n);
 /* Simulated time the drives are evaluated at (advanced by every step). */
 rp_status rp_batch_set_time(rp_batch* batch, double time);
+/* One waypoint schedule per rod (n = num_rods), replacing the sinusoidal
+ * drives of rp_batch_set_drives; the schedules' step count restarts at 0.
+ * NULL removes them. */
+rp_status rp_batch_set_waypoint_drives(rp_batch* batch, const rp_waypoint_drive* drives, int32_t n);
+/* Routing outcome of every rod's current centre line on `board`, computed on
+ * the device in double exactly as the reference evaluates downloaded float
+ * positions (HarnessTask::evaluate, harness_routing.cpp:108-154; called by
+ * attemptsOnGpu, application_cases.cpp:251-261, after a full
+ * downloadPositions). Only the n outcomes cross to the host. Synchronous. */
+rp_status rp_batch_evaluate_harness(rp_batch* batch, const rp_harness_board* board,
+                                    rp_harness_outcome* out, int32_t n);
 
 /* Raw asynchronous copies between the device state and caller memory, on
  * the batch's stream (no reference counterpart: the reference copies

@@ -449,6 +449,15 @@ class Reference:
         L.ref_hold_many.argtypes = [C.POINTER(vp), C.POINTER(vp), C.c_int, C.c_double, C.c_int, C.c_int,
                                     d3, C.c_int, C.c_int, C.c_int, d3, C.POINTER(C.c_int)]
         L.ref_contacts.argtypes = [vp, C.POINTER(C.c_int), d3, d3, d3, C.c_int]
+        L.ref_harness_steps.restype = C.c_int
+        L.ref_harness_hand_policy.argtypes = [d3]
+        L.ref_harness_velocity.argtypes = [d3, C.c_int, d3]
+        L.ref_harness_evaluate.argtypes = [C.POINTER(C.c_float), C.c_int, d3, C.POINTER(C.c_int)]
+        L.ref_harness_build.restype = vp
+        L.ref_harness_build.argtypes = [C.c_double]
+        L.ref_harness_world.restype = vp
+        L.ref_harness_world.argtypes = [C.c_double]
+        L.ref_harness_attempt_cpu.argtypes = [d3, C.c_double, C.c_double, d3, C.POINTER(C.c_int), d3]
         self.gpu = gpu
         if gpu:
             L.refgpu_create.restype = vp
@@ -468,6 +477,47 @@ class Reference:
             L.refgpu_overflow.argtypes = [vp]
             L.refgpu_self_pairs.argtypes = [vp, C.c_int, C.POINTER(C.c_int), C.c_int]
             L.refgpu_contact_active.argtypes = [vp, C.c_int, C.POINTER(C.c_int)]
+
+    # ---- the harness-routing task (src/apps/harness_routing.h:27-97) ----
+    @staticmethod
+    def _outcome(d, f):
+        return dict(score=d[0], side_a=d[1], side_b=d[2], clip_miss=d[3], below_a=bool(f[0]),
+                    above_b=bool(f[1]), through_clip=bool(f[2]), success=bool(f[3]))
+
+    def harness_hand_policy(self) -> np.ndarray:
+        p = np.zeros(10)
+        self.lib.ref_harness_hand_policy(p.ctypes.data_as(C.POINTER(C.c_double)))
+        return p.reshape(5, 2)
+
+    def harness_velocity(self, policy, step: int) -> np.ndarray:
+        """HarnessTask::gripperVelocity in double."""
+        p = np.ascontiguousarray(policy, np.float64).reshape(10)
+        v = np.zeros(3)
+        d3 = C.POINTER(C.c_double)
+        self.lib.ref_harness_velocity(p.ctypes.data_as(d3), int(step), v.ctypes.data_as(d3))
+        return v
+
+    def harness_evaluate(self, xyz) -> dict:
+        """HarnessTask::evaluate of one cable given as float positions."""
+        x = np.ascontiguousarray(xyz, np.float32).reshape(-1, 3)
+        d = np.zeros(4)
+        f = np.zeros(4, np.int32)
+        self.lib.ref_harness_evaluate(x.ctypes.data_as(C.POINTER(C.c_float)), len(x),
+                                      d.ctypes.data_as(C.POINTER(C.c_double)),
+                                      f.ctypes.data_as(C.POINTER(C.c_int)))
+        return self._outcome(d, f)
+
+    def harness_attempt_cpu(self, policy, youngs_scale: float, friction_scale: float):
+        """One attempt on the FP64 CPU solver (attemptOnCpu); (outcome, positions)."""
+        p = np.ascontiguousarray(policy, np.float64).reshape(10)
+        d = np.zeros(4)
+        f = np.zeros(4, np.int32)
+        x = np.zeros((121, 3))
+        d3 = C.POINTER(C.c_double)
+        self.lib.ref_harness_attempt_cpu(p.ctypes.data_as(d3), float(youngs_scale), float(friction_scale),
+                                         d.ctypes.data_as(d3), f.ctypes.data_as(C.POINTER(C.c_int)),
+                                         x.ctypes.data_as(d3))
+        return self._outcome(d, f), x
 
     def gpu_self_pairs(self, batch, rod=0, cap=4096):
         """(j, k) pairs of the reference GPU's last self-contact regeneration

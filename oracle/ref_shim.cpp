@@ -2,7 +2,8 @@
 //
 // TEST INFRASTRUCTURE ONLY. Compiled by oracle/Makefile together with the
 // reference's source files where they lie (src/core/*.cpp, src/apps/
-// cable_hanging.cpp, and for the GPU variant src/gpu/gpu_solver.cu and
+// cable_hanging.cpp, src/apps/harness_routing.cpp, and for the GPU variant
+// src/gpu/gpu_solver.cu and
 // src/gpu/gpu_batch.cpp), into oracle/_ref/. Nothing from the reference is
 // copied into this repository; this file only calls its public API:
 //   crs::Rod, makeStraightRod, makeRodFromCenterline, clampEndExact
@@ -11,6 +12,7 @@
 //   crs::CollisionWorld, generateContacts, selfCollisionIndexGap
 //     (src/core/collision.h:83-121)
 //   crs::colorStretchConstraints / colorBendConstraints (src/core/coloring.h:41-42)
+//   crs::apps::HarnessTask (src/apps/harness_routing.h:27-97)
 //   crs::gpu::Batch (src/gpu/gpu_solver.h:66-145), when REF_WITH_GPU is set.
 // Rods cross the boundary as orc_rod views (oracle/rod_oracle.h) in double.
 #include <algorithm>
@@ -20,6 +22,7 @@
 #include <vector>
 
 #include "apps/cable_hanging.h"
+#include "apps/harness_routing.h"
 #include "core/coloring.h"
 #include "core/collision.h"
 #include "core/rod.h"
@@ -513,5 +516,88 @@ int refgpu_contact_active(void* bp, int rod, int* active) {
 }
 int refgpu_available() { return gpu::cudaAvailable() ? 1 : 0; }
 #endif
+
+
+// ---- the harness-routing task (src/apps/harness_routing.h:27-97) ----
+
+namespace {
+static apps::HarnessTask::Policy harnessPolicy(const double* p10) {
+    apps::HarnessTask::Policy pol;
+    for (int k = 0; k < apps::HarnessTask::kWaypoints; ++k) pol[k] = Vec3(p10[2 * k], p10[2 * k + 1], 0);
+    return pol;
+}
+static void harnessOutcome(const apps::HarnessTask::Outcome& o, double* d4, int* f4) {
+    d4[0] = o.score;
+    d4[1] = o.sideA;
+    d4[2] = o.sideB;
+    d4[3] = o.clipMiss;
+    f4[0] = o.belowA;
+    f4[1] = o.aboveB;
+    f4[2] = o.throughClip;
+    f4[3] = o.success();
+}
+}  // namespace
+
+int ref_harness_steps() { return apps::HarnessTask().steps(); }
+
+void ref_harness_hand_policy(double* p10) {
+    const auto pol = apps::HarnessTask().handWrittenPolicy();
+    for (int k = 0; k < apps::HarnessTask::kWaypoints; ++k) {
+        p10[2 * k] = pol[k].x;
+        p10[2 * k + 1] = pol[k].y;
+    }
+}
+
+// HarnessTask::gripperVelocity(policy, step) (harness_routing.cpp:101-106).
+void ref_harness_velocity(const double* p10, int step, double* v3) {
+    const Vec3 v = apps::HarnessTask().gripperVelocity(harnessPolicy(p10), step);
+    v3[0] = v.x;
+    v3[1] = v.y;
+    v3[2] = v.z;
+}
+
+// HarnessTask::evaluate over float positions widened to double, as
+// attemptsOnGpu does (application_cases.cpp:251-261).
+void ref_harness_evaluate(const float* xyz, int numParticles, double* d4, int* f4) {
+    std::vector<Vec3> cable(numParticles);
+    for (int i = 0; i < numParticles; ++i)
+        cable[i] = Vec3(Real(xyz[3 * i]), Real(xyz[3 * i + 1]), Real(xyz[3 * i + 2]));
+    harnessOutcome(apps::HarnessTask().evaluate(cable), d4, f4);
+}
+
+void* ref_harness_build(double youngsScale) {
+    auto* h = new RodHandle;
+    h->rod = apps::HarnessTask().build(Real(youngsScale));
+    return h;
+}
+
+void* ref_harness_world(double frictionScale) {
+    auto* w = new WorldHandle;
+    w->world = apps::HarnessTask().world(Real(frictionScale));
+    return w;
+}
+
+// One attempt on the FP64 CPU solver in the GPU's colour order
+// (attemptOnCpu, application_cases.cpp:264-278); positions out (3 per particle).
+void ref_harness_attempt_cpu(const double* p10, double youngsScale, double frictionScale, double* d4,
+                             int* f4, double* xyz) {
+    const apps::HarnessTask task;
+    Rod rod = task.build(Real(youngsScale));
+    const CollisionWorld world = task.world(Real(frictionScale));
+    const Coloring stretch = colorStretchConstraints(rod);
+    const Coloring bend = colorBendConstraints(rod);
+    SolverParams p = task.params();
+    p.stretchColoring = &stretch;
+    p.bendColoring = &bend;
+    SolverContext ctx;
+    const auto pol = harnessPolicy(p10);
+    for (int s = 0; s < task.steps(); ++s) {
+        rod.state.kinematicVelocity.back() = task.gripperVelocity(pol, s);
+        step(rod, p, world, ctx);
+    }
+    harnessOutcome(task.evaluate(rod.state.x), d4, f4);
+    if (xyz)
+        for (std::size_t i = 0; i < rod.state.x.size(); ++i) put3(xyz, int(i), rod.state.x[i]);
+}
 
 }  // extern "C"

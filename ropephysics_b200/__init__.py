@@ -26,7 +26,7 @@ from . import _abi
 __all__ = ["RopeError", "Strategy", "Precision", "ContactState", "Material", "Primitive", "World",
            "StepParams", "Drive", "Rod", "Batch", "Server", "cuda_available", "device_name",
            "diagnostic", "max_fused_segments", "coloring", "self_collision_index_gap", "lib", "Trajectory",
-           "read_rodtraj"]
+           "read_rodtraj", "WaypointDrive", "HarnessBoard", "HARNESS_OUTCOME"]
 
 
 def lib():
@@ -175,6 +175,39 @@ class Drive:
     frequency: float = 0.0
     phase: float = 0.0
 
+
+@dataclass
+class WaypointDrive:
+    """On-device waypoint schedule of one pinned particle (a gripper motion):
+    from `start` through `waypoints` (x, y), `legs` seconds each with a
+    smoothstep, at `height`, the velocity held for `steps_per_control`
+    steps of `dt` (rp_waypoint_drive)."""
+    particle: int
+    start: Sequence[float]
+    waypoints: Sequence[Sequence[float]]
+    legs: Sequence[float]
+    height: float = 0.0
+    dt: float = 1e-3
+    steps_per_control: int = 1
+
+
+@dataclass
+class HarnessBoard:
+    """A routing board: the cable passes below peg A, above peg B and
+    through the clip (rp_harness_board)."""
+    peg_a: Sequence[float]
+    peg_b: Sequence[float]
+    clip: Sequence[float]
+    peg_radius: float
+    clip_half_gap: float
+    clip_height: float
+    cable_radius: float
+    lay_slack: float = 0.015
+
+
+HARNESS_OUTCOME = np.dtype([("score", "<f8"), ("side_a", "<f8"), ("side_b", "<f8"), ("clip_miss", "<f8"),
+                            ("below_a", "u1"), ("above_b", "u1"), ("through_clip", "u1"), ("success", "u1"),
+                            ("reserved", "u1", 4)])
 
 _F64 = C.POINTER(C.c_double)
 _I32 = C.POINTER(C.c_int32)
@@ -491,6 +524,50 @@ class Batch:
         _check(lib().rp_batch_set_material_scales(self._h, y.ctypes.data_as(FP) if y is not None else None,
                                                   f.ctypes.data_as(FP) if f is not None else None,
                                                   self.num_rods))
+
+    def set_waypoint_drives(self, drives: Optional[Sequence[Optional[WaypointDrive]]]):
+        """One waypoint schedule per rod (None: undriven rod); replaces the
+        sinusoidal drives and restarts the schedules' step count."""
+        if drives is None:
+            _check(lib().rp_batch_set_waypoint_drives(self._h, None, 0))
+            return
+        arr = (_abi.WaypointDrive * len(drives))()
+        for i, d in enumerate(drives):
+            if d is None:
+                arr[i].particle = -1
+                continue
+            n = len(d.waypoints)
+            if not 1 <= n <= _abi.MAX_WAYPOINTS or len(d.legs) != n:
+                raise ValueError(f"1..{_abi.MAX_WAYPOINTS} waypoints, one leg each")
+            arr[i].particle = d.particle
+            arr[i].count = n
+            arr[i].steps_per_control = d.steps_per_control
+            arr[i].dt = d.dt
+            arr[i].start[:] = [float(d.start[0]), float(d.start[1])]
+            arr[i].height = d.height
+            for k in range(n):
+                arr[i].legs[k] = float(d.legs[k])
+                arr[i].waypoints[k][0] = float(d.waypoints[k][0])
+                arr[i].waypoints[k][1] = float(d.waypoints[k][1])
+        _check(lib().rp_batch_set_waypoint_drives(self._h, arr, len(drives)))
+
+    def evaluate_harness(self, board: HarnessBoard) -> np.ndarray:
+        """Routing outcome of every rod's current centre line on `board`,
+        computed on the device (structured array, HARNESS_OUTCOME)."""
+        b = _abi.HarnessBoard()
+        b.peg_a[:] = [float(v) for v in board.peg_a[:2]]
+        b.peg_b[:] = [float(v) for v in board.peg_b[:2]]
+        b.clip[:] = [float(v) for v in board.clip[:2]]
+        b.peg_radius = board.peg_radius
+        b.clip_half_gap = board.clip_half_gap
+        b.clip_height = board.clip_height
+        b.cable_radius = board.cable_radius
+        b.lay_slack = board.lay_slack
+        out = np.zeros(self.num_rods, HARNESS_OUTCOME)
+        _check(lib().rp_batch_evaluate_harness(self._h, C.byref(b),
+                                               out.ctypes.data_as(C.POINTER(_abi.HarnessOutcome)),
+                                               self.num_rods))
+        return out
 
     def set_drives(self, drives: Optional[Sequence[Drive]]):
         if drives is None:

@@ -57,6 +57,27 @@ class Drive(C.Structure):
                 ("frequency", f32), ("phase", f32)]
 
 
+MAX_WAYPOINTS = 8
+
+
+class WaypointDrive(C.Structure):
+    _fields_ = [("particle", i32), ("count", i32), ("steps_per_control", i32), ("reserved", i32),
+                ("dt", C.c_double), ("start", C.c_double * 2), ("height", C.c_double),
+                ("legs", C.c_double * MAX_WAYPOINTS), ("waypoints", (C.c_double * 2) * MAX_WAYPOINTS)]
+
+
+class HarnessBoard(C.Structure):
+    _fields_ = [("peg_a", C.c_double * 2), ("peg_b", C.c_double * 2), ("clip", C.c_double * 2),
+                ("peg_radius", C.c_double), ("clip_half_gap", C.c_double), ("clip_height", C.c_double),
+                ("cable_radius", C.c_double), ("lay_slack", C.c_double)]
+
+
+class HarnessOutcome(C.Structure):
+    _fields_ = [("score", C.c_double), ("side_a", C.c_double), ("side_b", C.c_double),
+                ("clip_miss", C.c_double), ("below_a", C.c_uint8), ("above_b", C.c_uint8),
+                ("through_clip", C.c_uint8), ("success", C.c_uint8), ("reserved", C.c_uint8 * 4)]
+
+
 class ServerConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_uint64), ("params", StepParams), ("precision", i32),
                 ("max_steps_in_flight", i32)]
@@ -125,6 +146,8 @@ SIGNATURES = {
     "rp_batch_set_material_scales": (i32, [vp, P(f32), P(f32), i32]),
     "rp_batch_set_drives": (i32, [vp, P(Drive), i32]),
     "rp_batch_set_time": (i32, [vp, f64]),
+    "rp_batch_set_waypoint_drives": (i32, [vp, P(WaypointDrive), i32]),
+    "rp_batch_evaluate_harness": (i32, [vp, P(HarnessBoard), P(HarnessOutcome), i32]),
     "rp_batch_read_state_async": (i32, [vp, i32, vp, i64]),
     "rp_batch_write_state_async": (i32, [vp, i32, vp, i64]),
     "rp_batch_read_contact_states": (i32, [vp, P(u8), i64, P(i64)]),

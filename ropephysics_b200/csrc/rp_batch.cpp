@@ -83,6 +83,9 @@ struct rp_batch {
 
     std::vector<void*> owned;
     DArgs a{};
+    rp::DDrive* driveStore = nullptr;          // sinusoidal drives, kept while waypoints are in use
+    rp::DWaypoints* waypointStore = nullptr;   // waypoint schedules, kept while drives are in use
+    rp::DOutcome* outcomes = nullptr;          // harness evaluation output
     int32_t* dWork = nullptr;
 
     // batched plan
@@ -873,6 +876,7 @@ struct StateSnapshot {
         add(A.errors, R * 4);
         add(A.rodTime, R * 8);
         add(A.hold, R * sizeof(rp::DHold));
+        add(A.waypoints, R * sizeof(rp::DWaypoints));  // their step counters advance
         for (auto& rg : regions) {
             void* c = nullptr;
             if (cudaMalloc(&c, rg.second) != cudaSuccess) {
@@ -1221,18 +1225,106 @@ rp_status rp_batch_set_drives(rp_batch* b, const rp_drive* drives, int32_t n) {
         d[r].omega = float(2.0 * 3.14159265358979323846 * double(drives[r].frequency));
         d[r].phase = drives[r].phase;
     }
-    rp::DDrive* dd = const_cast<rp::DDrive*>(b->a.drives);
+    rp::DDrive* dd = b->driveStore;
     if (!dd) {
         rp_status st = b->alloc(dd, size_t(n));
         if (st != RP_OK) return st;
+        b->driveStore = dd;
     }
     rp_status st = b->upload(dd, d);
     if (st != RP_OK) return st;
     b->a.drives = dd;
+    b->a.waypoints = nullptr;  // one kind of drive at a time
     if (b->graphExec) {
         cudaGraphExecDestroy(b->graphExec);
         b->graphExec = nullptr;
     }
+    return syncBatch(b);
+}
+
+rp_status rp_batch_set_waypoint_drives(rp_batch* b, const rp_waypoint_drive* drives, int32_t n) {
+    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
+    auto dropGraph = [&]() {
+        if (b->graphExec) {
+            cudaGraphExecDestroy(b->graphExec);
+            b->graphExec = nullptr;
+        }
+    };
+    if (!drives) {
+        if (b->a.waypoints) dropGraph();
+        b->a.waypoints = nullptr;
+        return RP_OK;
+    }
+    if (n != b->numRods) return fail(RP_ERR_INVALID, "n must equal num_rods");
+    static_assert(rp::kMaxWaypoints == RP_MAX_WAYPOINTS, "waypoint capacity");
+    std::vector<rp::DWaypoints> w(n);
+    for (int r = 0; r < n; ++r) {
+        const rp_waypoint_drive& d = drives[r];
+        rp::DWaypoints& o = w[r];
+        o.particle = d.particle;
+        o.count = d.count;
+        o.stepsPerControl = d.steps_per_control;
+        o.step = 0;
+        o.dt = d.dt;
+        o.sx = d.start[0];
+        o.sy = d.start[1];
+        o.z = d.height;
+        if (d.particle >= b->tmplNP[r]) return fail(RP_ERR_INVALID, "waypoint drive particle out of range");
+        if (d.particle < 0) continue;
+        if (d.count < 1 || d.count > RP_MAX_WAYPOINTS)
+            return fail(RP_ERR_INVALID, "waypoint count must be 1.." + std::to_string(RP_MAX_WAYPOINTS));
+        if (d.steps_per_control < 1) return fail(RP_ERR_INVALID, "steps_per_control must be >= 1");
+        if (!(d.dt > 0) || !std::isfinite(d.dt)) return fail(RP_ERR_INVALID, "waypoint dt must be > 0");
+        for (int k = 0; k < RP_MAX_WAYPOINTS; ++k) {
+            const bool used = k < d.count;
+            if (used && (!(d.legs[k] > 0) || !std::isfinite(d.legs[k])))
+                return fail(RP_ERR_INVALID, "waypoint legs must be > 0");
+            o.legs[k] = used ? d.legs[k] : 0.0;
+            o.wx[k] = used ? d.waypoints[k][0] : 0.0;
+            o.wy[k] = used ? d.waypoints[k][1] : 0.0;
+        }
+    }
+    rp::DWaypoints* dw = b->waypointStore;
+    if (!dw) {
+        rp_status st = b->alloc(dw, size_t(n));
+        if (st != RP_OK) return st;
+        b->waypointStore = dw;
+    }
+    rp_status st = b->upload(dw, w);
+    if (st != RP_OK) return st;
+    // a captured graph holds the step arguments: it stays valid while they
+    // point at the same arrays, whose contents the kernels read at run time
+    if (b->a.waypoints != dw || b->a.drives) dropGraph();
+    b->a.waypoints = dw;
+    b->a.drives = nullptr;  // one kind of drive at a time
+    return syncBatch(b);
+}
+
+rp_status rp_batch_evaluate_harness(rp_batch* b, const rp_harness_board* board, rp_harness_outcome* out,
+                                    int32_t n) {
+    if (!b || !board || !out) return fail(RP_ERR_INVALID, "batch, board or out is NULL");
+    if (n != b->numRods) return fail(RP_ERR_INVALID, "n must equal num_rods");
+    static_assert(sizeof(rp_harness_outcome) == sizeof(rp::DOutcome), "outcome layout");
+    rp::DBoard B;
+    B.ax = board->peg_a[0];
+    B.ay = board->peg_a[1];
+    B.bx = board->peg_b[0];
+    B.by = board->peg_b[1];
+    B.cx = board->clip[0];
+    B.cy = board->clip[1];
+    B.pegRadius = board->peg_radius;
+    B.clipHalfGap = board->clip_half_gap;
+    B.clipHeight = board->clip_height;
+    B.radius = board->cable_radius;
+    B.slack = board->lay_slack;
+    if (!b->outcomes) {
+        rp_status st = b->alloc(b->outcomes, size_t(b->numRods), false);
+        if (st != RP_OK) return st;
+    }
+    const int comp = (b->precision & RP_PRECISION_COMPENSATED) != 0;
+    RP_CUDA(rp::launchEvaluateHarness(b->a, B, comp, b->outcomes, b->stream));
+    RP_CUDA(cudaMemcpyAsync(out, b->outcomes, size_t(n) * sizeof(rp::DOutcome), cudaMemcpyDeviceToHost,
+                            b->stream));
     return syncBatch(b);
 }
 

@@ -256,6 +256,14 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
         drive = A.drives[r];
         if (drive.particle >= 0 && drive.particle < nP) driveP = drive.particle;
     }
+    int wayP = -1, wayStep = 0;  // waypoint schedule: its particle and step count
+    if (A.waypoints) {
+        const DWaypoints& W = A.waypoints[r];
+        if (W.particle >= 0 && W.particle < nP) {
+            wayP = W.particle;
+            wayStep = W.step;
+        }
+    }
 
     // ---- stage in (coalesced float4 rows) ----
     {
@@ -290,6 +298,7 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
     const int stepsHere = A.stepsPerLaunch > 0 ? A.stepsPerLaunch : 1;
     for (int step = 0; step < stepsHere; ++step) {
         if (driveP >= 0 && lane == 0) V.kin[driveP] = driveVelocityB(drive, tRod);
+        if (wayP >= 0 && lane == 0) V.kin[wayP] = waypointVelocity(A.waypoints[r], wayStep + step);
         teamSync(team, teamIdx);
         for (int sub = 0; sub < A.substeps; ++sub) {
             for (int k = lane; k < nSt; k += team) V.lamS[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -595,6 +604,7 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
     if (lane == 0) {
         if (self) A.selfCount[r] = *S.live;
         A.rodTime[r] = tRod;
+        if (wayP >= 0) A.waypoints[r].step = wayStep + stepsHere;
     }
 }
 

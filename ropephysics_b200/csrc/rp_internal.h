@@ -81,6 +81,27 @@ struct DDrive {
     float pad;
 };
 
+// Waypoint schedule of a pinned particle (rp_waypoint_drive); `step` counts
+// the steps taken since the schedule was set and is advanced by the kernels.
+constexpr int kMaxWaypoints = 8;
+struct DWaypoints {
+    int32_t particle, count, stepsPerControl, step;
+    double dt, sx, sy, z;
+    double legs[kMaxWaypoints];
+    double wx[kMaxWaypoints], wy[kMaxWaypoints];
+};
+
+// Routing board and outcome (rp_harness_board, rp_harness_outcome).
+struct DBoard {
+    double ax, ay, bx, by, cx, cy;
+    double pegRadius, clipHalfGap, clipHeight, radius, slack;
+};
+struct DOutcome {
+    double score, sideA, sideB, clipMiss;
+    uint8_t belowA, aboveB, throughClip, success;
+    uint8_t reserved[4];
+};
+
 // Hold/slide observer state per rod (HangOutcome, cable_hanging.h:68-77).
 struct DHold {
     int32_t particle;   // < 0: not armed
@@ -146,6 +167,7 @@ struct DArgs {
     int32_t* errors;        // per rod: error bits set by the kernels (0 = none)
     double* rodTime;        // per rod simulated time (drives)
     const DDrive* drives;   // per rod, may be null
+    DWaypoints* waypoints;  // per rod, may be null (step counters advance)
     DHold* hold;            // per rod, may be null
     int32_t holdInterval;
 

@@ -35,6 +35,10 @@ cudaError_t staticScratch(void** ptr, size_t* bytes);
 // xyz of n particles packed as 3 floats each (compensated: x - xComp).
 cudaError_t launchPackPositions(const float4* x, const float4* xComp, float* out, int64_t n, cudaStream_t stream);
 
+// Routing outcome of every rod on a harness board (one warp per rod).
+cudaError_t launchEvaluateHarness(const DArgs& a, const DBoard& board, int compensated, DOutcome* out,
+                                  cudaStream_t stream);
+
 // One hold observation of every armed rod (the final sample of a run).
 cudaError_t launchObserve(const DArgs& a, int compensated, cudaStream_t stream);
 

@@ -156,6 +156,15 @@ __global__ void __launch_bounds__(128, 4) kPlainStep(DArgs A) {
             driveV = driveVelocity(d, A.rodTime[r]);
         }
     }
+    bool waypointDriven = false;
+    if (A.waypoints) {
+        const DWaypoints& W = A.waypoints[r];
+        if (W.particle >= 0 && W.particle < nP) {
+            driveP = W.particle;
+            driveV = waypointVelocity(W, W.step);
+            waypointDriven = true;
+        }
+    }
 
     // ---- stage in ----
     if (!GMEM) {
@@ -287,6 +296,7 @@ __global__ void __launch_bounds__(128, 4) kPlainStep(DArgs A) {
             A.selfOverflow[r] += *S.overflow;
         }
         A.rodTime[r] += double(A.dt);
+        if (waypointDriven) A.waypoints[r].step += 1;  // every thread read it before the first barrier
         if (A.hold) {
             DHold& H = A.hold[r];
             if (H.particle >= 0 && H.particle < nP) {

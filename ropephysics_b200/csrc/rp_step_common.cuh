@@ -629,4 +629,42 @@ __device__ __forceinline__ void finishFrame(const RodView& V, int j, float h, fl
     V.omega[j] = f4(im(dq) * (2.0f / h) * angDecay);
 }
 
+// ---------------------------------------------------------------- waypoint drives
+
+// Position of a waypoint schedule at time t (reference HarnessTask::gripperAt,
+// harness_routing.cpp:81-99), in double with every operation rounded
+// separately (no contraction), as the host code computes it.
+__device__ __forceinline__ void waypointAt(const DWaypoints& W, double t, double& px, double& py) {
+    double fx = W.sx, fy = W.sy, t0 = 0.0;
+    for (int k = 0; k < W.count; ++k) {
+        const double t1 = __dadd_rn(t0, W.legs[k]);
+        if (t < t1) {
+            double u = __ddiv_rn(__dsub_rn(t, t0), W.legs[k]);
+            u = __dmul_rn(__dmul_rn(u, u), __dsub_rn(3.0, __dmul_rn(2.0, u)));
+            px = __dadd_rn(fx, __dmul_rn(__dsub_rn(W.wx[k], fx), u));
+            py = __dadd_rn(fy, __dmul_rn(__dsub_rn(W.wy[k], fy), u));
+            return;
+        }
+        fx = W.wx[k];
+        fy = W.wy[k];
+        t0 = t1;
+    }
+    px = fx;
+    py = fy;
+}
+
+// Kinematic velocity during step `step` (reference HarnessTask::gripperVelocity,
+// harness_routing.cpp:101-106): the control tick's displacement times the
+// reciprocal of its period (the reference's vector division), as floats.
+__device__ __forceinline__ float4 waypointVelocity(const DWaypoints& W, int step) {
+    const double period = __dmul_rn(W.dt, double(W.stepsPerControl));
+    const int tick = step / W.stepsPerControl;
+    double ax, ay, bx, by;
+    waypointAt(W, __dmul_rn(double(tick + 1), period), ax, ay);
+    waypointAt(W, __dmul_rn(double(tick), period), bx, by);
+    const double inv = __ddiv_rn(1.0, period);
+    return make_float4(float(__dmul_rn(__dsub_rn(ax, bx), inv)), float(__dmul_rn(__dsub_rn(ay, by), inv)),
+                       float(__dmul_rn(__dsub_rn(W.z, W.z), inv)), 0.0f);
+}
+
 }  // namespace rp
