@@ -465,10 +465,30 @@ rp_status buildBatchedPlan(rp_batch* b) {
     std::vector<int32_t> ids(b->numRods), order;
     for (int r = 0; r < b->numRods; ++r) ids[r] = r;
     const int cta = b->tune.ctaThreads;
-    const size_t maxSmem = rpx::planGroups(ids, b->rods.data(), b->tmpls.data(), cta, b->tune.pairsPerThread,
-                                           (b->precision & RP_PRECISION_COMPENSATED) != 0, order, b->groups);
-    b->numGroups = int(b->groups.size() / 4);
+    const bool comp = (b->precision & RP_PRECISION_COMPENSATED) != 0;
     const size_t optin = optinSmem(b->device);
+    // World contact slots go into shared memory when the groups still fit as
+    // many CTAs per SM with them (few contact primitives per rod, or short
+    // rods); otherwise they stay in global memory.
+    size_t maxSmem = rpx::planGroups(ids, b->rods.data(), b->tmpls.data(), cta, b->tune.pairsPerThread, comp,
+                                     order, b->groups, false);
+    b->a.slotsShared = 0;
+    if (b->maxPrims > 0) {
+        std::vector<int32_t> order2, groups2;
+        const size_t smem2 = rpx::planGroups(ids, b->rods.data(), b->tmpls.data(), cta, b->tune.pairsPerThread,
+                                             comp, order2, groups2, true);
+        int per1 = 0, per2 = 0;
+        if (smem2 + 1024 <= optin && rp::batchedReserveSmem(std::max(smem2, maxSmem)) == cudaSuccess &&
+            rp::batchedOccupancy(cta, maxSmem, &per1) == cudaSuccess &&
+            rp::batchedOccupancy(cta, smem2, &per2) == cudaSuccess && per2 >= per1 && per2 >= 1) {
+            maxSmem = smem2;
+            order.swap(order2);
+            b->groups.swap(groups2);
+            b->a.slotsShared = 1;
+        }
+        cudaGetLastError();
+    }
+    b->numGroups = int(b->groups.size() / 4);
     if (maxSmem + 1024 > optin)  // the kernel also has a few bytes of static shared memory
         return fail(RP_ERR_SHARED_MEMORY, "a rod group needs " + std::to_string(maxSmem) +
                                               " bytes of shared memory; the device allows " +

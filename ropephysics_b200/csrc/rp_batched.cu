@@ -204,7 +204,7 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
     V.contactMargin = R.contactMargin;
 
     const RodLayout L = rodLayout(nP, nS, nSt, nB, R.numPrims, R.selfCollision, R.hashTableSize,
-                                  R.selfCapacity, 1, COMP ? 1 : 0);
+                                  R.selfCapacity, 1, COMP ? 1 : 0, A.slotsShared);
     V.q = reinterpret_cast<float4*>(base + L.q);
     V.qPrev = COMP ? A.gqPrev + R.sOff : reinterpret_cast<float4*>(base + L.qPrev);
     V.x = reinterpret_cast<float4*>(base + L.x);
@@ -219,7 +219,7 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
     V.torque = A.torque + R.sOff;
     V.lamS = reinterpret_cast<float4*>(base + L.lamS);
     V.lamB = reinterpret_cast<float4*>(base + L.lamB);
-    V.slots = A.gSlots + R.slotOff;
+    V.slots = A.slotsShared ? reinterpret_cast<DSlot*>(base + L.slots) : A.gSlots + R.slotOff;
     SelfScratch S;
     S.centres = reinterpret_cast<float4*>(base + L.centres);
     S.cellOf = reinterpret_cast<int32_t*>(base + L.selfInt);
@@ -629,7 +629,8 @@ __global__ void __launch_bounds__(256, 2) kBatchedStep(DArgs A, const int32_t* _
                 const DRod Rk = A.rods[A.work[first + k]];
                 const DTemplate Tk = A.tmpl[Rk.tmpl];
                 off += size_t(rodLayout(Tk.nP, Tk.nS, Tk.nSt, Tk.nB, Rk.numPrims, Rk.selfCollision,
-                                        Rk.hashTableSize, Rk.selfCapacity, 1, COMP ? 1 : 0).bytes);
+                                        Rk.hashTableSize, Rk.selfCapacity, 1, COMP ? 1 : 0, A.slotsShared)
+                                  .bytes);
             }
             runRod<COMP, FP64>(A, A.work[first + teamIdx], smem + off, lane, team, teamIdx);
         }

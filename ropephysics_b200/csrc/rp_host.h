@@ -54,7 +54,7 @@ void makeTemplate(const rp_rod_desc* d, TemplateHost& out);
 int teamThreads(int nSt, int pairsPerThread);
 size_t planGroups(const std::vector<int32_t>& rodIds, const rp::DRod* rods, const rp::DTemplate* tmpls,
                   int cta, int pairsPerThread, bool comp, std::vector<int32_t>& order,
-                  std::vector<int32_t>& groups);
+                  std::vector<int32_t>& groups, bool slotsShared = false);
 
 // ---- rp_batch.cpp: what the trajectory writer reads of a batch ----
 struct BatchView {

@@ -205,7 +205,7 @@ int teamThreads(int nSt, int pairsPerThread) {
 // shared bytes.
 size_t planGroups(const std::vector<int32_t>& rodIds, const rp::DRod* rods, const rp::DTemplate* tmpls,
                   int cta, int pairsPerThread, bool comp, std::vector<int32_t>& order,
-                  std::vector<int32_t>& groups) {
+                  std::vector<int32_t>& groups, bool slotsShared) {
     order = rodIds;
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
         return tmpls[rods[x].tmpl].nSt > tmpls[rods[y].tmpl].nSt;
@@ -225,7 +225,8 @@ size_t planGroups(const std::vector<int32_t>& rodIds, const rp::DRod* rods, cons
             const rp::DTemplate& T = tmpls[R.tmpl];
             if (std::min(cta, teamThreads(T.nSt, pairsPerThread)) != team) break;
             const rp::RodLayout L = rp::rodLayout(T.nP, T.nS, T.nSt, T.nB, R.numPrims, R.selfCollision,
-                                                  R.hashTableSize, R.selfCapacity, 1, comp ? 1 : 0);
+                                                  R.hashTableSize, R.selfCapacity, 1, comp ? 1 : 0,
+                                                  slotsShared ? 1 : 0);
             smem += size_t(L.bytes);
             ++cnt;
         }

@@ -168,6 +168,7 @@ struct DArgs {
     double* rodTime;        // per rod simulated time (drives)
     const DDrive* drives;   // per rod, may be null
     DWaypoints* waypoints;  // per rod, may be null (step counters advance)
+    int32_t slotsShared;    // batched: world contact slots in shared memory
     DHold* hold;            // per rod, may be null
     int32_t holdInterval;
 

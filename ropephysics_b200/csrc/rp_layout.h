@@ -10,13 +10,16 @@
 // hash -- and leaves in global memory what a step only reads (loads,
 // kinematic velocities) or touches only when a contact is live (world
 // contact slots of primitives that survive the per-rod cull, the
-// self-contact pool); those stay L1/L2-resident.
+// self-contact pool); those stay L1/L2-resident. `slotsShared` moves the
+// world contact slots into the lean layout too, for batches whose groups
+// still fit as many CTAs per SM with them.
 //   frames     q, qPrev (not lean+comp), omega [, torque]  16 x nS each
 //   particles  x, xPrev, v [, force, kin], xComp     16 x nP each (xComp: full,
 //                                                    or lean with compensation)
 //   frames     qComp                                 16 x nS (lean with compensation)
 //   lambdas    stretch, bend                         16 x (nSt + nB)
-//   slots      [world contacts]                      32 x nP x numPrims
+//   slots      [world contacts]                      32 x nP x numPrims (full, or lean
+//                                                    with slotsShared)
 //   misc       kMiscBytes (below)
 //   self       centres 16 nSt, ints 16 nSt, hash + cursor 2 x 4 (table + 1),
 //              [pool 64 x capacity], projection levels 3 x 4 (capacity + 1),
@@ -53,7 +56,7 @@ RP_HD inline int32_t rpAlign16(int32_t b) { return (b + 15) & ~15; }
 
 RP_HD inline RodLayout rodLayout(int32_t nP, int32_t nS, int32_t nSt, int32_t nB, int32_t nPrims,
                                  int32_t self, int32_t table, int32_t capacity, int32_t lean = 0,
-                                 int32_t comp = 0) {
+                                 int32_t comp = 0, int32_t slotsShared = 0) {
     RodLayout L;
     int32_t o = 0;
     L.q = o;      o += 16 * nS;
@@ -85,7 +88,7 @@ RP_HD inline RodLayout rodLayout(int32_t nP, int32_t nS, int32_t nSt, int32_t nB
     }
     L.lamS = o;   o += 16 * nSt;
     L.lamB = o;   o += 16 * nB;
-    if (!lean) {
+    if (!lean || slotsShared) {
         L.slots = o;  o += 32 * nP * nPrims;
     } else {
         L.slots = -1;
