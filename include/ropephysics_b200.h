@@ -69,12 +69,23 @@ typedef enum rp_strategy {
  *                             renormalised in FP64 once per substep; uploads
  *                             keep the double inputs' rounding residuals).
  *   RP_PRECISION_FP64_CONE    the Coulomb stick/slip cap test in FP64.
- *   RP_PRECISION_FP64_VERDICT near-boundary hold/slide classification in FP64. */
+ *   RP_PRECISION_FP64_VERDICT near-boundary hold/slide classification in FP64.
+ *   RP_PRECISION_COLORED_SELF the self-contact pool projected colour by colour
+ *                             (greedy colours over shared particles) instead
+ *                             of in the reference's serial pool order: the
+ *                             reference's proposed speed-up for its serial
+ *                             self-contact loop (REMAINING.md:14-17). A
+ *                             different Gauss-Seidel order, so results differ
+ *                             from every other mode; batched strategy only
+ *                             (the fused and multi-kernel strategies keep the
+ *                             serial order); a pool needing more than 32
+ *                             colours keeps the exact level order. */
 typedef enum rp_precision {
     RP_PRECISION_REFERENCE = 0,
     RP_PRECISION_COMPENSATED = 1,
     RP_PRECISION_FP64_CONE = 2,
-    RP_PRECISION_FP64_VERDICT = 4
+    RP_PRECISION_FP64_VERDICT = 4,
+    RP_PRECISION_COLORED_SELF = 8
 } rp_precision;
 
 /* Primitive types (reference: TPrimitive::Type, geometry.h:19). */

@@ -55,6 +55,7 @@ class Precision(enum.IntFlag):
     COMPENSATED = 1
     FP64_CONE = 2
     FP64_VERDICT = 4
+    COLORED_SELF = 8
 
 
 class ContactState(enum.IntEnum):

@@ -806,7 +806,8 @@ rp_status rp_batch_set_stream(rp_batch* b, void* stream) {
 
 rp_status rp_batch_set_precision(rp_batch* b, int32_t flags) {
     if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
-    if (flags & ~7) return fail(RP_ERR_INVALID, "unknown precision flag");
+    static_assert(rp::kPrecisionColoredSelf == RP_PRECISION_COLORED_SELF, "precision flag");
+    if (flags & ~15) return fail(RP_ERR_INVALID, "unknown precision flag");
     if ((flags & RP_PRECISION_COMPENSATED) != (b->precision & RP_PRECISION_COMPENSATED)) {
         // entering or leaving compensated mode: the compensation starts at zero
         RP_CUDA(cudaMemsetAsync(b->a.xComp, 0, size_t(b->totalP) * sizeof(float4), b->stream));

@@ -459,8 +459,22 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
                         teamSync(team, teamIdx);
                         if (lane == 0) {
                             int kept = live;
-                            *numLevels = buildProjectionLevels(S.pool, live, nP, S.cellOf, lvlOf, lvlOrder,
-                                                               lvlStart, &kept);
+                            int n = buildProjectionLevels(S.pool, live, nP, S.cellOf, lvlOf, lvlOrder,
+                                                          lvlStart, &kept);
+                            if (A.precision & kPrecisionColoredSelf) {
+                                // colours instead of levels (the valid prefix is known now)
+                                for (int i = 0; i < nP; ++i) S.cellOf[i] = 0;
+                                const int nc = buildProjectionColors(S.pool, kept, S.cellOf, lvlOf, lvlOrder,
+                                                                     lvlStart);
+                                if (nc >= 0) {
+                                    n = nc;
+                                } else {  // more than 32 colours: keep the levels
+                                    for (int i = 0; i < nP; ++i) S.cellOf[i] = 0;
+                                    n = buildProjectionLevels(S.pool, kept, nP, S.cellOf, lvlOf, lvlOrder,
+                                                              lvlStart, &kept);
+                                }
+                            }
+                            *numLevels = n;
                             if (kept != live) {
                                 // an entry indexed outside the rod or left unwritten:
                                 // keep the valid prefix and report it, never touch

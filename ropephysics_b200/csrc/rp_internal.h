@@ -83,6 +83,9 @@ struct DDrive {
 
 // Waypoint schedule of a pinned particle (rp_waypoint_drive); `step` counts
 // the steps taken since the schedule was set and is advanced by the kernels.
+// RP_PRECISION_COLORED_SELF, as the kernels test it in DArgs::precision.
+constexpr int32_t kPrecisionColoredSelf = 8;
+
 constexpr int kMaxWaypoints = 8;
 struct DWaypoints {
     int32_t particle, count, stepsPerControl, step;

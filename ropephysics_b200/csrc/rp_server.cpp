@@ -459,7 +459,7 @@ rp_status rp_server_create(const rp_server_config* cfg, rp_server** out) {
     if (cfg->hbm_budget_bytes < (1u << 20)) return fail(RP_ERR_INVALID, "budget below 1 MiB");
     const rp_step_params& p = cfg->params;
     if (!(p.dt > 0) || p.substeps < 1 || p.iterations < 0) return fail(RP_ERR_INVALID, "bad step params");
-    if (cfg->precision & ~7) return fail(RP_ERR_INVALID, "unknown precision flag");
+    if (cfg->precision & ~15) return fail(RP_ERR_INVALID, "unknown precision flag");
     std::string why;
     if (!rpx::deviceUsable(&why)) return fail(RP_ERR_NO_DEVICE, why);
     auto* s = new rp_server();

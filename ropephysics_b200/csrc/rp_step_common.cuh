@@ -532,6 +532,40 @@ __device__ __forceinline__ int buildProjectionLevels(const DSelf* pool, int live
     return levels;
 }
 
+// Greedy colours for projecting a self-contact pool in parallel (the
+// reference's proposed speed-up for its serial self-contact loop,
+// REMAINING.md:14-17): in pool order, each contact takes the lowest colour
+// that none of its four particles has taken yet. A colour's contacts touch
+// disjoint particles, so a colour projects in parallel exactly as in any
+// order; the colours run in ascending order. This is a different
+// Gauss-Seidel order from the serial loop's, so results differ from it (the
+// levels above reproduce it). `used` holds one zeroed int per particle (a
+// bitmask of its colours), `colOf` one int per contact; fills order/start as
+// buildProjectionLevels does and returns the number of colours, or -1 when a
+// contact would need a 33rd colour (`used` is then dirty). The first `live`
+// entries must be valid (buildProjectionLevels' prefix check). One thread.
+__device__ __forceinline__ int buildProjectionColors(const DSelf* pool, int live, int32_t* used,
+                                                     int32_t* colOf, int32_t* order, int32_t* start) {
+    int colors = 0;
+    for (int c = 0; c < live; ++c) {
+        const DSelf& k = pool[c];
+        unsigned m = 0u;
+        for (int q = 0; q < 4; ++q) m |= unsigned(used[k.idx[q]]);
+        if (m == 0xffffffffu) return -1;
+        const int col = __ffs(~m) - 1;
+        colOf[c] = col;
+        for (int q = 0; q < 4; ++q) used[k.idx[q]] = int32_t(unsigned(used[k.idx[q]]) | (1u << col));
+        colors = max(colors, col + 1);
+    }
+    for (int l = 0; l <= colors; ++l) start[l] = 0;
+    for (int c = 0; c < live; ++c) ++start[colOf[c] + 1];
+    for (int l = 0; l < colors; ++l) start[l + 1] += start[l];
+    for (int c = 0; c < live; ++c) order[start[colOf[c]]++] = c;
+    for (int l = colors; l > 0; --l) start[l] = start[l - 1];
+    start[0] = 0;
+    return colors;
+}
+
 // The four-particle case of the contact projection.
 template <bool COMP>
 __device__ __forceinline__ void projectSelf(const RodView& V, DSelf& c) {
