@@ -33,11 +33,17 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# Floating-point operations per segment-substep of the plain step (add, sub,
-# mul, div, sqrt), counted exactly by the op-counting oracle build
-# (liboracle_count.so; tests/test_oracle.py pins these values). Contacts add
-# ~10 per (particle, primitive) slot.
-FLOPS_PER_SEG_SUBSTEP = {"grid": 890.5, "uneven": 880.5, "cantilever": 880.5, "hook": 890.5}
+# Floating-point operations (add, sub, mul, div, sqrt) per segment-substep of
+# the reference's step, counted by the op-counting oracle build
+# (liboracle_count.so; tests/test_oracle.py recomputes every value):
+#   uneven      32 sampled rods of the uneven batch (seed 0), steps 25-44 -- the
+#               window a 5-warm-up, 20-step run times -- with their primitives
+#               and self-collision (contacts and self-contacts included)
+#   hook        16 placements spread over the hook sweep, steps 23-42 (the
+#               window the shape timing measures), bar, floor, self-collision
+#   grid        a pinned 64-segment rod over the floor plane
+#   cantilever  a pinned 64-segment rod, no contacts
+FLOPS_PER_SEG_SUBSTEP = {"uneven": 1696.2, "hook": 1463.8, "grid": 890.5, "cantilever": 880.5}
 # Algorithmic HBM bytes per segment per step: state read once and written once
 # (x, v, force, kinematic velocity per particle; q, omega, torque per frame;
 # float4 rows): read 4 x 16 + 3 x 16, written 2 x 16 + 2 x 16.
@@ -156,69 +162,138 @@ def build_workload(name: str, rods: int, seed: int):
 # ----------------------------------------------------------------------------- CPU reference
 
 
-def cpu_reference_rate(wl, sample_rods: int, budget_s: float, threads: int):
-    """The reference's own FP64 CPU step (src/core/solver.cpp, compiled from its
-    sources into oracle/_ref) on a bounded sample of the same workload, rods
-    spread over host threads as its throughput case does
-    (src/validation/scaling_cases.cpp:404-459). Falls back to this
-    repository's restatement (oracle/liboracle_f64.so) when the reference
-    library is absent. Returns (rate, kind, sample description, threads)."""
-    import oracle as orc
-    kind = "reference"
-    try:
-        ref = orc.Reference(gpu=False)
-    except FileNotFoundError:
-        ref = None
-        kind = "port"
-    rng = np.random.default_rng(123)
-    idx = rng.choice(len(wl.rods), size=min(sample_rods, len(wl.rods)), replace=False)
-    p = wl.params
-    f32 = lambda v: float(np.float32(v))
-    params = orc.Params(dt=f32(p.dt), substeps=p.substeps, iterations=p.iterations,
-                        gravity=tuple(f32(g) for g in p.gravity))
-    segs = sum(wl.rods[i].num_stretch for i in idx)
-    if ref is not None:
-        handles, worlds = [], []
-        for i in idx:
-            r = wl.rods[i]
-            h = ref.centerline(r.x, youngs=r.material.youngs, poisson=r.material.poisson,
-                               density=r.material.density, radius=r.material.radius)
-            rr = ref.export(h)
-            n = r.num_particles
-            rr.x[:n] = r.x
-            rr.invMass[:n] = r.inv_mass
-            rr.q[: r.num_frames] = r.q
-            rr.bRestD[: r.num_bend] = r.b_rest_darboux
-            rr.kinVel[:n] = r.kin_velocity
-            rr.extForce[:n] = r.ext_force
-            ref.import_state(h, rr)
-            handles.append(h)
-            w = wl.worlds[wl.world_of_rod[i]] if wl.worlds else None
-            worlds.append(ref.world(orc.World([orc.Primitive(q.type, q.a, q.b, q.normal, q.half_extents,
-                                                             q.rotation, q.radius, q.friction)
-                                               for q in w.primitives], w.self_collision,
-                                              w.self_friction, w.self_skip, w.hash_table_size,
-                                              w.contact_margin_radii)) if w else None)
-        H = (C.c_void_p * len(handles))(*handles)
-        W = (C.c_void_p * len(worlds))(*worlds)
-        g = (C.c_double * 3)(*params.gravity)
+def load_synth():
+    """ropephysics_b200/synth.py loaded by its path: the workload's seeded
+    draws without importing the package, so a CPU-only process never maps the
+    library."""
+    import importlib.util
+    name = "ropephysics_b200_synth"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, os.path.join(ROOT, "ropephysics_b200", "synth.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
 
-        def run(steps):
-            return ref.lib.ref_step_many(H, W, len(handles), params.dt, params.substeps,
-                                         params.iterations, g, 0.0, 0.0, 1, steps, threads)
-        t1 = run(1)
-        steps = max(1, min(200, int(budget_s / max(t1, 1e-3))))
-        t = run(steps)
-        for h in handles:
-            ref.free(h)
+
+WORKLOAD_PARAMS = {"uneven": (1.0 / 60, 50), "grid": (1.0 / 60, 20), "cantilever": (1.0 / 60, 20)}
+
+
+def workload_config(name: str, rods: int, seed: int) -> dict:
+    """The workload's description, computed from the draws alone, identical in
+    both arms' JSON lines."""
+    S = load_synth()
+    dt, substeps = WORKLOAD_PARAMS[name]
+    if name == "uneven":
+        n = rods or 16384
+        segs = sum(d.segments for d in S.uneven(n, seed))
+        wname = f"uneven-{n}x[16,512]"
+    elif name == "grid":
+        n = rods or 4096
+        segs, wname = 64 * n, f"grid-{n}x64"
     else:
-        o = orc.Oracle("f64")
-        rods = [orc.Rod(wl.rods[i].num_particles) for i in idx]
-        raise SystemExit("reference CPU library missing and port path not wired")
-    rate = segs * p.substeps * steps / t
-    sample = (f"{len(idx)} of {len(wl.rods)} rods ({segs} segments) x {steps} steps x "
-              f"{p.substeps} substeps, {t:.1f} s")
-    return rate, kind, sample, threads
+        n, segs, wname = 1, 64, "cantilever-1x64"
+    state_bytes = BYTES_PER_SEG_STEP * segs
+    return {"workload": wname, "rods": n, "segments": int(segs), "substeps": substeps, "dt": dt,
+            "l2": "inputs larger than L2" if state_bytes > 126e6 else "L2-resident state"}
+
+
+class ReferenceSample:
+    """A bounded sample of the workload built by the reference's own builders
+    (makeRodFromCenterline / makeStraightRod, src/core/rod.cpp) and stepped
+    by its own FP64 CPU solver (crs::step, src/core/solver.cpp:269-290) in the
+    GPU colour order, both compiled from the reference's sources into
+    oracle/_ref/libcrs_ref.so. Rods are spread over host threads in contiguous
+    ranges, as the reference's throughput case does
+    (src/validation/scaling_cases.cpp:404-459). The rods come from the same
+    seeded draws as the GPU arm's (ropephysics_b200/synth.py)."""
+
+    def __init__(self, name: str, rods: int, seed: int, sample_rods: int):
+        import oracle as orc
+        S = load_synth()
+        self.ref = ref = orc.Reference(gpu=False)
+        self.handles, self.worlds = [], []
+        mat = dict(youngs=S.YOUNGS, poisson=S.POISSON, density=S.DENSITY, radius=S.RADIUS)
+        rng = np.random.default_rng(123)
+        if name == "uneven":
+            draws = S.uneven(rods or 16384, seed)
+            idx = rng.choice(len(draws), size=min(sample_rods, len(draws)), replace=False)
+            for i in idx:
+                d = draws[i]
+                h = ref.centerline(d.points, frame_seed=(0.0, 0.0, 1.0), **mat)
+                rr = ref.export(h)
+                rr.bRestD[:] = 0.0  # straight rest shape: the coil is loaded
+                ref.import_state(h, rr)
+                self.handles.append(h)
+                self.worlds.append(ref.world(orc.World([orc.Primitive(*q) for q in d.prims], True, d.friction,
+                                                       2, d.hash_table_size, 0.25)))
+            self.segments = int(sum(draws[i].segments for i in idx))
+            total = len(draws)
+        elif name == "grid":
+            g = S.grid(rods or 4096, seed)
+            idx = rng.choice(len(g.youngs_scale), size=min(sample_rods, len(g.youngs_scale)), replace=False)
+            for i in idx:
+                m = dict(mat, youngs=S.YOUNGS * float(g.youngs_scale[i]))
+                h = ref.straight(64, 1.0, origin=(0.0, 0.0, 0.0), direction=(0.0, 0.0, -1.0), **m)
+                rr = ref.export(h)
+                rr.invMass[0] = 0.0  # pinned top, moving at its drive's t = 0 velocity
+                w = 2 * math.pi * g.frequency[i]
+                rr.kinVel[0] = (0.0, 0.0, g.amplitude[i] * w * math.cos(g.phase[i]))
+                ref.import_state(h, rr)
+                self.handles.append(h)
+                mu = 0.5 * float(g.friction_scale[i])
+                self.worlds.append(ref.world(orc.World([orc.Primitive(*S.plane((0.0, 0.0, -1.2),
+                                                                               (0.0, 0.0, 1.0), mu))])))
+            self.segments = 64 * len(idx)
+            total = len(g.youngs_scale)
+        else:
+            h = ref.straight(64, 1.0, **mat)
+            ref.lib.ref_rod_clamp(h, 0)
+            rr = ref.export(h)
+            rr.extForce[rr.nP - 1] = (0.0, 0.0, -0.05)
+            ref.import_state(h, rr)
+            self.handles.append(h)
+            self.worlds.append(None)
+            self.segments, total, idx = 64, 1, [0]
+        dt, self.substeps = WORKLOAD_PARAMS[name]
+        f32 = lambda v: float(np.float32(v))
+        self.params = orc.Params(dt=f32(dt), substeps=self.substeps, iterations=1,
+                                 gravity=(0.0, 0.0, f32(-9.81)))
+        self.desc = f"{len(idx)} of {total} rods ({self.segments} segments)"
+
+    def run(self, steps: int, threads: int) -> float:
+        """Wall seconds of `steps` steps of every sampled rod."""
+        p = self.params
+        H = (C.c_void_p * len(self.handles))(*self.handles)
+        W = (C.c_void_p * len(self.worlds))(*self.worlds)
+        g = (C.c_double * 3)(*p.gravity)
+        return self.ref.lib.ref_step_many(H, W, len(self.handles), p.dt, p.substeps, p.iterations, g, 0.0, 0.0,
+                                          1, steps, threads)
+
+    def close(self):
+        for h in self.handles:
+            self.ref.free(h)
+        self.handles = []
+
+
+def cpu_reference_rate(name: str, rods: int, seed: int, sample_rods: int, budget_s: float, threads: int,
+                       advance: int):
+    """The reference's FP64 CPU step on a bounded sample of the workload, over
+    `threads` host threads, timed from step `advance` (the step the GPU's
+    timed region starts at: a coil's contact work changes as it relaxes).
+    Returns (rate, kind, sample description, threads)."""
+    sample = ReferenceSample(name, rods, seed, sample_rods)
+    if advance > 1:
+        sample.run(advance - 1, threads)
+    t1 = sample.run(1, threads)
+    steps = max(1, min(200, int(budget_s / max(t1, 1e-3))))
+    t = sample.run(steps, threads)
+    sample.close()
+    rate = sample.segments * sample.substeps * steps / t
+    desc = (f"{sample.desc} x {steps} steps x {sample.substeps} substeps from step {advance}, "
+            f"{t:.1f} s")
+    return rate, "reference", desc, threads
 
 
 # ----------------------------------------------------------------------------- served stream
@@ -401,12 +476,18 @@ def run_ours(args):
     import ropephysics_b200 as rp
 
     wl = build_workload(args.workload, args.rods, seed=args.seed + rank)
+    config = workload_config(args.workload, args.rods, args.seed + rank)
+    config["parallelism"] = f"replicas{world_size}"
+    assert config["segments"] == int(wl.segments.sum()) and config["workload"] == wl.name
     seg_sub = wl.segment_substeps_per_step()
+    p = wl.params
+    # the roofline denominator, measured on this device before anything else runs
+    fp32_peak = rp.measure_fp32_peak(8192)
+
     batch = wl.make_batch(rp.Strategy.BATCHED)
     stream = torch.cuda.Stream()
     batch.set_stream(stream.cuda_stream)
     batch.set_graph(True)
-    p = wl.params
     # rods per CTA, threads per rod and steps per launch, timed on this batch
     # (its state is restored afterwards)
     tuning = batch.autotune(p, max_steps_per_launch=4) if not args.no_tune else batch.tuning
@@ -416,6 +497,15 @@ def run_ours(args):
         batch.step_many(p, 1)
     batch.step_many(p, args.steps)
     batch.synchronize()
+    # the end-to-end twin: the same rods, advanced to the state the timed
+    # region starts from (every launch shape gives bitwise the same steps)
+    twin = None
+    if not args.no_e2e:
+        twin = wl.make_batch(rp.Strategy.BATCHED)
+        twin.set_stream(stream.cuda_stream)
+        twin.set_tuning(tuning["cta_threads"], tuning["pairs_per_thread"], 1)
+        twin.step_many(p, args.warmup + args.steps)
+        twin.synchronize()
 
     # ---- device-resident throughput (value) ----
     barrier(world_size)
@@ -434,32 +524,40 @@ def run_ours(args):
     value = seg_sub * args.steps * world_size / (ms / 1e3)
 
     # ---- end to end through the public API with pinned host buffers ----
-    nbytes = {k: batch.state_bytes(k) for k in (batch.POSITIONS, batch.FRAMES, batch.CONTACTS)}
-    kin = torch.zeros(batch.total_particles * 4, dtype=torch.float32).pin_memory()
-    outs = {k: torch.empty(max(1, n), dtype=torch.uint8).pin_memory() for k, n in nbytes.items()}
-    e2e_steps = max(3, args.steps // 2)
-    batch.set_graph(False)
-
-    def e2e_step():
-        batch.write_state_async(batch.KINEMATIC, kin.data_ptr(), 16 * batch.total_particles)
-        batch.step(p)
-        for k, n in nbytes.items():
-            if n:
-                batch.read_state_async(k, outs[k].data_ptr(), n)
-        batch.synchronize()
-    e2e_step()
-    barrier(world_size)
-    torch.cuda.synchronize()
-    # events on the batch's stream bracket the copies and the steps; every
-    # step ends in a host synchronize, so the span includes the host round trips
-    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    f0.record(stream)
-    for _ in range(e2e_steps):
-        e2e_step()
-    f1.record(stream)
-    f1.synchronize()
-    e2e_s = max_over_ranks(f0.elapsed_time(f1) / 1e3, world_size)
-    e2e = seg_sub * e2e_steps * world_size / e2e_s
+    # Every step: the kinematic velocities in (host -> device), one step, the
+    # positions, frames and contact states out (device -> host), then a host
+    # synchronize. Same rods and same starting state as the timed region.
+    e2e = None
+    if twin is not None:
+        nbytes = {k: twin.state_bytes(k) for k in (twin.POSITIONS, twin.FRAMES, twin.CONTACTS)}
+        h2d = 16 * twin.total_particles
+        kin = torch.zeros(twin.total_particles * 4, dtype=torch.float32).pin_memory()
+        outs = {k: torch.empty(max(1, n), dtype=torch.uint8).pin_memory() for k, n in nbytes.items()}
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+        barrier(world_size)
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            ev[k][0].record(stream)
+            twin.write_state_async(twin.KINEMATIC, kin.data_ptr(), h2d)
+            ev[k][1].record(stream)
+            twin.step(p)
+            ev[k][2].record(stream)
+            for what, n in nbytes.items():
+                if n:
+                    twin.read_state_async(what, outs[what].data_ptr(), n)
+            ev[k][3].record(stream)
+            twin.synchronize()
+        phase = [sum(ev[k][i].elapsed_time(ev[k][i + 1]) for k in range(args.steps)) / args.steps
+                 for i in range(3)]
+        e2e_s = max_over_ranks(ev[0][0].elapsed_time(ev[-1][3]) / 1e3, world_size)
+        d2h = int(sum(nbytes.values()))
+        e2e = {"value": seg_sub * args.steps * world_size / e2e_s, "unit": "segment-substeps/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "ms_per_step": e2e_s * 1e3 / args.steps,
+               "h2d_ms": phase[0], "step_ms": phase[1], "d2h_ms": phase[2],
+               "h2d_gbs": h2d / phase[0] / 1e6, "d2h_gbs": d2h / phase[2] / 1e6,
+               "start": "the timed region's starting state (twin batch)"}
+        twin.close()
 
     # ---- plain one-rod-per-CTA step on the same batch (batched vs plain) ----
     plain_rate = None
@@ -482,12 +580,14 @@ def run_ours(args):
             plain_rate = f"unavailable: {e}"
 
     peaks = measured_peaks()
-    per_launch_s = (ms / 1e3) / args.steps
-    flops = FLOPS_PER_SEG_SUBSTEP.get(args.workload, 880.5) * seg_sub
-    bytes_alg = BYTES_PER_SEG_STEP * int(wl.segments.sum())
+    per_launch_s = (ms / 1e3) / max(1, launches)
+    steps_per_launch = args.steps / max(1, launches)
+    fps = FLOPS_PER_SEG_SUBSTEP.get(args.workload, 880.5)
+    flops_launch = fps * seg_sub * steps_per_launch
+    bytes_launch = BYTES_PER_SEG_STEP * config["segments"] * steps_per_launch
+    traffic = (DRAM_BYTES_PER_SEG_STEP[args.workload] * config["segments"] * steps_per_launch
+               if args.workload in DRAM_BYTES_PER_SEG_STEP else None)
     clk = clocks.summary()
-    sms = torch.cuda.get_device_properties(local).multi_processor_count
-    fp32_peak = sms * 128 * 2 * (clk.get("sm_max_mhz") or 1965.0) * 1e6 / 1e12
     line = {
         "metric": "segment-substeps/s",
         "value": value,
@@ -501,36 +601,38 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded)",
-        "config": {"workload": wl.name, "rods": len(wl.rods), "segments": int(wl.segments.sum()),
-                   "substeps": p.substeps, "dt": p.dt, "strategy": "batched", "tuning": tuning,
-                   "graph": True, "l2": "inputs larger than L2" if bytes_alg > 126e6 else "L2-resident state",
-                   "parallelism": f"replicas{world_size}"},
-        "e2e": {"value": e2e, "unit": "segment-substeps/s", "h2d_bytes_per_step": 16 * batch.total_particles,
-                "d2h_bytes_per_step": int(sum(nbytes.values()))},
+        "config": config,
+        "launch": {"strategy": "batched", "tuning": tuning, "graph": True,
+                   "steps_per_launch": steps_per_launch},
+        "e2e": e2e,
         "gpu_launches": int(launches),
         "plain": {"value": plain_rate, "unit": "segment-substeps/s",
                   "speedup": (value / world_size / plain_rate) if isinstance(plain_rate, float) else None},
-        "roofline": {"bound": "hbm", "achieved": bytes_alg / per_launch_s / 1e9,
-                     "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
-                     "frac": bytes_alg / per_launch_s / 1e9 / peaks.get("hbm_gbs", 6650.0),
-                     "traffic": (DRAM_BYTES_PER_SEG_STEP[args.workload] * int(wl.segments.sum())
-                                 if args.workload in DRAM_BYTES_PER_SEG_STEP else None),
-                     "note": "of measured; traffic per launch from ncu on 4096 rods scaled by segments; "
-                             "the step is FP32-latency bound, see fp32"},
-        "fp32": {"achieved": flops / per_launch_s / 1e12, "peak": fp32_peak, "unit": "TFLOP/s",
-                 "frac": flops / per_launch_s / 1e12 / fp32_peak,
-                 "flops_per_segment_substep": FLOPS_PER_SEG_SUBSTEP.get(args.workload, 880.5)},
+        "roofline": {"bound": "fp32", "achieved": flops_launch / per_launch_s / 1e12,
+                     "peak": fp32_peak["tflops"], "unit": "TFLOP/s",
+                     "frac": flops_launch / per_launch_s / 1e12 / fp32_peak["tflops"],
+                     "traffic": traffic,
+                     "flops_per_segment_substep": fps,
+                     "note": "of measured: peak = FP32 FMA microkernel on this GPU (rp_measure_fp32_peak); "
+                             "FLOPs = the reference step's add/sub/mul/div/sqrt count on this workload "
+                             "(op-counting oracle, contacts and self-collision included); traffic = DRAM "
+                             "bytes per launch from ncu on 4096 rods, scaled by segments"},
+        "hbm": {"achieved": bytes_launch / per_launch_s / 1e9, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                "frac": bytes_launch / per_launch_s / 1e9 / peaks.get("hbm_gbs", 6650.0),
+                "bytes_per_segment_step": BYTES_PER_SEG_STEP,
+                "peak_source": "fallback" if peaks.get("fallback") else "measured"},
         "clocks": clk,
     }
-    if not args.no_shapes:
-        line["shapes"] = measure_shapes(stream, fp32_peak)
-    if not args.no_served:
+    if world_size == 1 and not args.no_shapes:
+        line["shapes"] = measure_shapes(stream, fp32_peak["tflops"])
+    if world_size == 1 and not args.no_served:
         batch.close()
-        line["served"] = run_served(value / world_size, args.served_seconds, args.seed + 7 + rank,
+        line["served"] = run_served(value, args.served_seconds, args.seed + 7,
                                     args.served_load, args.served_budget_gb)
     if rank == 0 and world_size == 1 and not args.no_cpu:
-        rate, kind, sample, threads = cpu_reference_rate(wl, args.cpu_rods, args.cpu_seconds,
-                                                          os.cpu_count() or 1)
+        rate, kind, sample, threads = cpu_reference_rate(args.workload, args.rods, args.seed, args.cpu_rods,
+                                                          args.cpu_seconds, os.cpu_count() or 1,
+                                                          args.warmup + args.steps)
         line["cpu_baseline"] = {"value": rate, "unit": "segment-substeps/s", "cores": threads,
                                 "kind": kind, "sample": sample}
     if rank == 0:
@@ -542,31 +644,37 @@ def run_ours(args):
 
 
 def run_reference(args):
+    """The reference's own FP64 CPU step on this box's host cores, on the
+    workload's seeded draws: this process never imports ropephysics_b200.
+    Each timed step is one run of the bounded sample."""
     world_size = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    wl = build_workload(args.workload, args.rods, seed=args.seed)
+    config = workload_config(args.workload, args.rods, args.seed)
+    config["parallelism"] = f"replicas{world_size}"
     threads = os.cpu_count() or 1
-    rates = []
-    samples = []
-    for _ in range(args.warmup):
-        cpu_reference_rate(wl, args.cpu_rods, 1.0, threads)
-    for _ in range(max(1, args.steps)):
-        r, kind, sample, _ = cpu_reference_rate(wl, args.cpu_rods, args.cpu_seconds / max(1, args.steps),
-                                                threads)
-        rates.append(r)
-        samples.append(sample)
-    value = statistics.median(rates)
+    sample = ReferenceSample(args.workload, args.rods, args.seed, args.cpu_rods)
+    # warm-up: advance the sample to the step the GPU arm's timed region
+    # starts at (its warm-up steps plus its graph warm-up of `steps` steps)
+    sample.run(max(1, args.warmup + args.steps), threads)
+    steps = max(1, args.steps)
+    # steps of the sample per timed step, so the whole run takes ~cpu_seconds
+    t1 = sample.run(1, threads)
+    per = max(1, min(200, int(args.cpu_seconds / steps / max(t1, 1e-3))))
+    times = [sample.run(per, threads) for _ in range(steps)]
+    sample.close()
+    total = sum(times)
+    value = sample.segments * sample.substeps * per * steps / total
+    desc = (f"{sample.desc} x {per} steps x {sample.substeps} substeps per timed step, "
+            f"{steps} timed steps from step {args.warmup + args.steps}, {total:.1f} s")
     line = {"metric": "segment-substeps/s", "value": value, "unit": "segment-substeps/s",
-            "n_gpus": world_size, "steps": args.steps, "warmup": args.warmup,
+            "n_gpus": world_size, "steps": steps, "warmup": args.warmup,
+            "ms_per_step": total * 1e3 / steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded)", "impl": "reference",
-            "config": {"workload": wl.name, "rods": len(wl.rods), "segments": int(wl.segments.sum()),
-                       "substeps": wl.params.substeps, "dt": wl.params.dt,
-                       "parallelism": f"replicas{world_size}", "sample": "bounded CPU sample per step"},
+            "data": "synthetic (seeded)", "impl": "reference", "config": config,
             "cpu_baseline": {"value": value, "unit": "segment-substeps/s", "cores": threads,
-                             "kind": kind, "sample": samples[-1]},
+                             "kind": "reference", "sample": desc},
             "e2e": {"value": value, "unit": "segment-substeps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -585,10 +693,11 @@ def main():
     ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--no-shapes", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--cpu-rods", type=int, default=64)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-rods", type=int, default=256)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-served", action="store_true")
-    ap.add_argument("--served-seconds", type=float, default=20.0)
+    ap.add_argument("--served-seconds", type=float, default=60.0)
     ap.add_argument("--served-load", type=float, default=0.7)
     ap.add_argument("--served-budget-gb", type=float, default=150.0)
     args = ap.parse_args()

@@ -257,6 +257,13 @@ rp_status rp_diagnostic(char* out, size_t capacity);
 /* reference: maxFusedSegments(), gpu_solver.h:150 (here with the 227 KB
  * opt-in shared memory of sm_100, for a free rod without contacts). */
 int32_t rp_max_fused_segments(void);
+/* No reference counterpart. The current device's FP32 throughput, measured:
+ * a grid filling every SM runs `trips` x 128 independent fused multiply-adds
+ * per thread (two operations each), timed with CUDA events after one
+ * warm-up launch. Writes TFLOP/s to *tflops and the timed launch's
+ * milliseconds to *ms (may be NULL). The batched step is bound by FP32
+ * arithmetic, so this is its roofline denominator. */
+rp_status rp_measure_fp32_peak(int32_t trips, double* tflops, double* ms);
 /* Message of the last failure on the calling thread ("" if none). */
 const char* rp_last_error(void);
 int32_t rp_abi_version(void);
@@ -323,9 +330,12 @@ rp_status rp_batch_step_many(rp_batch* batch, const rp_step_params* params, int3
  * (work-queue counters, start-of-substep frames under compensated
  * precision, world-contact slots, self-contact pool) is carved from a fixed static device array of
  * RP_STATIC_SCRATCH_BYTES instead of the batch's own buffers, and the call
- * allocates no device memory. Needs: 256 + 16 x frames + 32 x contact slots
- * (+ 64 x self-contact pool entries), each section rounded up to 256 bytes;
- * a larger batch is rejected with RP_ERR_INVALID. The batch's device must be
+ * allocates no device memory. Needs 256 bytes, plus 16 x frames under
+ * RP_PRECISION_COMPENSATED, plus 32 x contact slots when the batch's plan
+ * keeps the slots in global memory (rods with many or large contact
+ * primitives), plus 64 x self-contact pool entries when any rod collides with
+ * itself, each section rounded up to 256 bytes; a larger batch is rejected
+ * with RP_ERR_INVALID. The batch's device must be
  * current. The first call on a device looks up the array's address, once;
  * make that first call before any stream capture. The queue counters are
  * cleared on the batch's stream before each launch; nothing else needs to

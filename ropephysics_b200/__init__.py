@@ -25,7 +25,7 @@ from . import _abi
 
 __all__ = ["RopeError", "Strategy", "Precision", "ContactState", "Material", "Primitive", "World",
            "StepParams", "Drive", "Rod", "Batch", "Server", "cuda_available", "device_name",
-           "diagnostic", "max_fused_segments", "coloring", "self_collision_index_gap", "lib", "Trajectory",
+           "diagnostic", "max_fused_segments", "measure_fp32_peak", "coloring", "self_collision_index_gap", "lib", "Trajectory",
            "read_rodtraj", "WaypointDrive", "HarnessBoard", "HARNESS_OUTCOME"]
 
 
@@ -364,6 +364,14 @@ def self_collision_index_gap(rod: Rod, world: World) -> int:
 
 def cuda_available() -> bool:
     return bool(lib().rp_cuda_available())
+
+
+def measure_fp32_peak(trips: int = 4096) -> dict:
+    """The current device's FP32 FMA throughput, measured on every SM
+    (rp_measure_fp32_peak): {"tflops": ..., "ms": ...}."""
+    t, ms = C.c_double(), C.c_double()
+    _check(lib().rp_measure_fp32_peak(int(trips), C.byref(t), C.byref(ms)))
+    return {"tflops": t.value, "ms": ms.value}
 
 
 def device_name() -> str:

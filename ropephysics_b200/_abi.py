@@ -112,6 +112,7 @@ SIGNATURES = {
     "rp_diagnostic": (i32, [C.c_char_p, C.c_size_t]),
     "rp_max_fused_segments": (i32, []),
     "rp_last_error": (C.c_char_p, []),
+    "rp_measure_fp32_peak": (i32, [i32, P(f64), P(f64)]),
     "rp_rod_create_straight": (i32, [i32, f64, P(Material), P(f64), P(f64), pp]),
     "rp_rod_create_centerline": (i32, [P(f64), i32, P(Material), P(f64), f64, pp]),
     "rp_rod_create_from_desc": (i32, [P(RodDesc), pp]),

@@ -28,7 +28,8 @@ INCLUDES = [f"-I{os.path.join(ROOT, 'include')}", f"-I{CSRC}", f"-I{os.path.join
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"] + ARCH
 CXX_FLAGS = ["-std=c++17", "-O3", "-fPIC", "-Wall", "-Wextra", "-Wno-unused-parameter"]
 
-CU_SOURCES = ["rp_plain.cu", "rp_batched.cu", "rp_static_scratch.cu", "rp_traj.cu", "rp_harness.cu"]
+CU_SOURCES = ["rp_plain.cu", "rp_batched.cu", "rp_static_scratch.cu", "rp_traj.cu", "rp_harness.cu",
+              "rp_peak.cu"]
 CPP_SOURCES = ["rp_rod.cpp", "rp_hostutil.cpp", "rp_batch.cpp", "rp_server.cpp", "rp_traj.cpp"]
 HEADERS = ["rp_internal.h", "rp_layout.h", "rp_launch.h", "rp_math.cuh", "rp_step_common.cuh",
            "rp_host.h"]

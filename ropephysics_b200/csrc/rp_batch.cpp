@@ -160,7 +160,7 @@ bool sameTopology(const rp_batch* b, int r, const rp_rod_desc* d) {
     return d && d->num_particles == b->tmplNP[r] && d->num_frames == b->tmplNS[r];
 }
 
-rp_status buildBatchedPlan(rp_batch* b);
+rp_status buildBatchedPlan(rp_batch* b, const Tune& tune, int precision);
 
 }  // namespace
 
@@ -449,7 +449,7 @@ static rp_status createImpl(const rp_rod_desc* const* rods, int numRods, const r
     }
 
     if (strategy == RP_STRATEGY_BATCHED) {
-        if ((st = buildBatchedPlan(b)) != RP_OK) return guard(st);
+        if ((st = buildBatchedPlan(b, b->tune, b->precision)) != RP_OK) return guard(st);
     }
     *out = b;
     return RP_OK;
@@ -459,70 +459,105 @@ static rp_status createImpl(const rp_rod_desc* const* rods, int numRods, const r
 
 namespace {
 
-rp_status buildBatchedPlan(rp_batch* b) {
+// Plans the batched launch for `tune` and `precision` and commits it only
+// when every step succeeded: on failure the batch keeps its previous plan,
+// device group table and work order untouched, so a refused change of
+// tuning or precision leaves a batch that still steps correctly.
+rp_status buildBatchedPlan(rp_batch* b, const Tune& tune, int precision) {
     // Length-sorted work order: longest first, so the tail of the persistent
     // queue is short rods and the SMs finish together.
-    std::vector<int32_t> ids(b->numRods), order;
+    std::vector<int32_t> ids(b->numRods), order, groups;
     for (int r = 0; r < b->numRods; ++r) ids[r] = r;
-    const int cta = b->tune.ctaThreads;
-    const bool comp = (b->precision & RP_PRECISION_COMPENSATED) != 0;
+    const int cta = tune.ctaThreads;
+    const bool comp = (precision & RP_PRECISION_COMPENSATED) != 0;
     const size_t optin = optinSmem(b->device);
     // World contact slots go into shared memory when the groups still fit as
     // many CTAs per SM with them (few contact primitives per rod, or short
     // rods); otherwise they stay in global memory.
-    size_t maxSmem = rpx::planGroups(ids, b->rods.data(), b->tmpls.data(), cta, b->tune.pairsPerThread, comp,
-                                     order, b->groups, false);
-    b->a.slotsShared = 0;
+    size_t maxSmem = rpx::planGroups(ids, b->rods.data(), b->tmpls.data(), cta, tune.pairsPerThread, comp,
+                                     order, groups, false);
+    int slotsShared = 0;
     if (b->maxPrims > 0) {
         std::vector<int32_t> order2, groups2;
-        const size_t smem2 = rpx::planGroups(ids, b->rods.data(), b->tmpls.data(), cta, b->tune.pairsPerThread,
+        const size_t smem2 = rpx::planGroups(ids, b->rods.data(), b->tmpls.data(), cta, tune.pairsPerThread,
                                              comp, order2, groups2, true);
         int per1 = 0, per2 = 0;
         if (smem2 + 1024 <= optin && rp::batchedReserveSmem(std::max(smem2, maxSmem)) == cudaSuccess &&
-            rp::batchedOccupancy(cta, maxSmem, &per1) == cudaSuccess &&
-            rp::batchedOccupancy(cta, smem2, &per2) == cudaSuccess && per2 >= per1 && per2 >= 1) {
+            rp::batchedOccupancy(cta, maxSmem, precision, &per1) == cudaSuccess &&
+            rp::batchedOccupancy(cta, smem2, precision, &per2) == cudaSuccess && per2 >= per1 && per2 >= 1) {
             maxSmem = smem2;
             order.swap(order2);
-            b->groups.swap(groups2);
-            b->a.slotsShared = 1;
+            groups.swap(groups2);
+            slotsShared = 1;
         }
         cudaGetLastError();
     }
-    b->numGroups = int(b->groups.size() / 4);
     if (maxSmem + 1024 > optin)  // the kernel also has a few bytes of static shared memory
         return fail(RP_ERR_SHARED_MEMORY, "a rod group needs " + std::to_string(maxSmem) +
                                               " bytes of shared memory; the device allows " +
                                               std::to_string(optin));
-    b->batchedSmem = maxSmem;
-    b->batchedThreads = cta;
     if (rp::batchedReserveSmem(std::max<size_t>(maxSmem, 1)) != cudaSuccess) {
         cudaGetLastError();
         return fail(RP_ERR_SHARED_MEMORY, "cannot opt into the batched shared memory");
     }
     int perSm = 0;
-    if (rp::batchedOccupancy(cta, maxSmem, &perSm) != cudaSuccess || perSm < 1) {
+    if (rp::batchedOccupancy(cta, maxSmem, precision, &perSm) != cudaSuccess || perSm < 1) {
         cudaGetLastError();
         return fail(RP_ERR_SHARED_MEMORY, "batched kernel cannot be resident with this group size");
     }
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
-    b->batchedBlocks = std::max(1, std::min(b->numGroups, sms * perSm));
-    if (!b->dWork) {
-        rp_status st;
-        if ((st = b->alloc(b->dWork, b->numRods)) != RP_OK) return st;
-        if ((st = b->alloc(b->dQueue, 2)) != RP_OK) return st;
-    }
-    if (b->dGroups) {
-        cudaFree(b->dGroups);
-        b->owned.erase(std::find(b->owned.begin(), b->owned.end(), static_cast<void*>(b->dGroups)));
-        b->dGroups = nullptr;
-    }
+    const int numGroups = int(groups.size() / 4);
     rp_status st;
-    if ((st = b->alloc(b->dGroups, b->groups.size())) != RP_OK) return st;
-    if ((st = b->upload(b->dWork, order)) != RP_OK) return st;
-    if ((st = b->upload(b->dGroups, b->groups)) != RP_OK) return st;
-    RP_CUDA(cudaStreamSynchronize(b->stream));
+    if (!b->dQueue && (st = b->alloc(b->dQueue, 2)) != RP_OK) return st;
+    // new device tables, filled before anything of the old plan is released
+    int32_t* newWork = nullptr;
+    int32_t* newGroups = nullptr;
+    auto drop = [&]() {
+        if (newWork) cudaFree(newWork);
+        if (newGroups) cudaFree(newGroups);
+        cudaGetLastError();
+    };
+    if (cudaMalloc(&newWork, std::max<size_t>(order.size(), 1) * sizeof(int32_t)) != cudaSuccess ||
+        cudaMalloc(&newGroups, std::max<size_t>(groups.size(), 1) * sizeof(int32_t)) != cudaSuccess) {
+        drop();
+        return fail(RP_ERR_OUT_OF_MEMORY, "cannot allocate the batched work tables");
+    }
+    cudaError_t e = cudaSuccess;
+    if (!order.empty())
+        e = cudaMemcpyAsync(newWork, order.data(), order.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                            b->stream);
+    if (e == cudaSuccess && !groups.empty())
+        e = cudaMemcpyAsync(newGroups, groups.data(), groups.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                            b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) {
+        drop();
+        return fail(RP_ERR_CUDA, std::string("batched work tables: ") + cudaGetErrorString(e));
+    }
+    // commit
+    if (b->graphExec) {  // a captured graph holds the old tables' addresses
+        cudaGraphExecDestroy(b->graphExec);
+        b->graphExec = nullptr;
+    }
+    for (void* old : {static_cast<void*>(b->dWork), static_cast<void*>(b->dGroups)}) {
+        if (!old) continue;
+        cudaFree(old);
+        b->owned.erase(std::find(b->owned.begin(), b->owned.end(), old));
+    }
+    b->dWork = newWork;
+    b->dGroups = newGroups;
+    b->owned.push_back(newWork);
+    b->owned.push_back(newGroups);
+    b->groups.swap(groups);
+    b->numGroups = numGroups;
+    b->a.slotsShared = slotsShared;
     b->a.work = b->dWork;
+    b->batchedSmem = maxSmem;
+    b->batchedThreads = cta;
+    b->batchedBlocks = std::max(1, std::min(numGroups, sms * perSm));
+    b->tune.ctaThreads = tune.ctaThreads;
+    b->tune.pairsPerThread = tune.pairsPerThread;
     return RP_OK;
 }
 
@@ -690,12 +725,17 @@ rp_status rp_batch_step_static_scratch(rp_batch* b, const rp_step_params* p) {
     RP_CUDA(cudaGetDevice(&dev));
     if (dev != b->device)
         return fail(RP_ERR_INVALID, "the batch's device (" + std::to_string(b->device) + ") must be current");
-    // scratch sections, 256-byte aligned: work-queue counters, start-of-substep
-    // frames, world-contact slots, self-contact pool
+    // scratch sections, 256-byte aligned, each only where the step reads it
+    // from global memory: work-queue counters; start-of-substep frames
+    // (compensated precision: otherwise they live in shared memory);
+    // world-contact slots (unless the plan keeps them in shared memory);
+    // self-contact pool (when a rod collides with itself)
     auto up = [](size_t n) { return (n + 255) & ~size_t(255); };
+    const bool comp = (b->precision & RP_PRECISION_COMPENSATED) != 0;
+    const bool globalSlots = b->a.slotsShared == 0 && b->totalSlots > 0;
     const size_t qPrevAt = 256;
-    const size_t slotsAt = qPrevAt + up(size_t(b->totalS) * sizeof(float4));
-    const size_t poolAt = slotsAt + up(size_t(b->totalSlots) * sizeof(rp::DSlot));
+    const size_t slotsAt = qPrevAt + (comp ? up(size_t(b->totalS) * sizeof(float4)) : 0);
+    const size_t poolAt = slotsAt + (globalSlots ? up(size_t(b->totalSlots) * sizeof(rp::DSlot)) : 0);
     const size_t need = poolAt + (b->anySelf ? up(size_t(b->totalPool) * sizeof(rp::DSelf)) : 0);
     void* base = nullptr;
     size_t have = 0;
@@ -709,8 +749,8 @@ rp_status rp_batch_step_static_scratch(rp_batch* b, const rp_step_params* p) {
     unsigned char* s = static_cast<unsigned char*>(base);
     DArgs A = b->a;
     fillStepArgs(b, p, A);
-    A.gqPrev = reinterpret_cast<float4*>(s + qPrevAt);
-    A.gSlots = reinterpret_cast<rp::DSlot*>(s + slotsAt);
+    A.gqPrev = comp ? reinterpret_cast<float4*>(s + qPrevAt) : nullptr;
+    A.gSlots = globalSlots ? reinterpret_cast<rp::DSlot*>(s + slotsAt) : nullptr;
     A.gPool = b->anySelf ? reinterpret_cast<rp::DSelf*>(s + poolAt) : nullptr;
     rp::BatchedPlan plan;
     plan.groups = b->dGroups;
@@ -809,15 +849,16 @@ rp_status rp_batch_set_precision(rp_batch* b, int32_t flags) {
     static_assert(rp::kPrecisionColoredSelf == RP_PRECISION_COLORED_SELF, "precision flag");
     if (flags & ~15) return fail(RP_ERR_INVALID, "unknown precision flag");
     if ((flags & RP_PRECISION_COMPENSATED) != (b->precision & RP_PRECISION_COMPENSATED)) {
+        // the batched layout keeps the compensation in shared memory: plan
+        // first, so a layout that no longer fits leaves the batch unchanged
+        if (b->strategy == RP_STRATEGY_BATCHED) {
+            rp_status st = syncBatch(b);
+            if (st != RP_OK) return st;
+            if ((st = buildBatchedPlan(b, b->tune, flags)) != RP_OK) return st;
+        }
         // entering or leaving compensated mode: the compensation starts at zero
         RP_CUDA(cudaMemsetAsync(b->a.xComp, 0, size_t(b->totalP) * sizeof(float4), b->stream));
         RP_CUDA(cudaMemsetAsync(b->a.qComp, 0, size_t(b->totalS) * sizeof(float4), b->stream));
-        b->precision = flags;
-        // the batched layout keeps the compensation in shared memory
-        if (b->strategy == RP_STRATEGY_BATCHED) {
-            rp_status st = buildBatchedPlan(b);
-            if (st != RP_OK) return st;
-        }
         if (b->graphExec) {
             cudaGraphExecDestroy(b->graphExec);
             b->graphExec = nullptr;
@@ -848,18 +889,14 @@ rp_status rp_batch_set_tuning(rp_batch* b, int32_t cta_threads, int32_t pairs_pe
         return fail(RP_ERR_INVALID, "steps_per_launch must be in 1..64");
     rp_status st = syncBatch(b);
     if (st != RP_OK) return st;
-    const Tune old = b->tune;
-    b->tune.ctaThreads = cta_threads;
-    b->tune.pairsPerThread = pairs_per_thread;
-    b->tune.stepsPerLaunch = steps_per_launch;
-    if (old.ctaThreads != cta_threads || old.pairsPerThread != pairs_per_thread) {
-        st = buildBatchedPlan(b);
-        if (st != RP_OK) {
-            b->tune = old;
-            const rp_status st2 = buildBatchedPlan(b);
-            return st2 != RP_OK ? st2 : st;
-        }
+    Tune want = b->tune;
+    want.ctaThreads = cta_threads;
+    want.pairsPerThread = pairs_per_thread;
+    want.stepsPerLaunch = steps_per_launch;
+    if (want.ctaThreads != b->tune.ctaThreads || want.pairsPerThread != b->tune.pairsPerThread) {
+        if ((st = buildBatchedPlan(b, want, b->precision)) != RP_OK) return st;  // batch unchanged
     }
+    b->tune = want;
     if (b->graphExec) {
         cudaGraphExecDestroy(b->graphExec);
         b->graphExec = nullptr;
@@ -956,10 +993,12 @@ rp_status rp_batch_autotune(rp_batch* b, const rp_step_params* p, int32_t max_st
     // plans, one warm launch and two timed launches from the same state
     for (int cta : {128, 256}) {
         for (int ppt : {1, 2}) {
-            b->tune.ctaThreads = cta;
-            b->tune.pairsPerThread = ppt;
+            Tune trialShape = start;
+            trialShape.ctaThreads = cta;
+            trialShape.pairsPerThread = ppt;
+            trialShape.stepsPerLaunch = 1;
+            if (buildBatchedPlan(b, trialShape, b->precision) != RP_OK) continue;
             b->tune.stepsPerLaunch = 1;
-            if (buildBatchedPlan(b) != RP_OK) continue;
             float ms = 0.0f;
             if ((st = snap.restore(b)) != RP_OK) break;
             if ((st = launchStep(b, p, 1)) != RP_OK) break;
@@ -975,8 +1014,7 @@ rp_status rp_batch_autotune(rp_batch* b, const rp_step_params* p, int32_t max_st
     // whole steps per launch, on the chosen shape; a longer launch must win
     // by 2 % to be kept
     if (st == RP_OK && bestMs < 3.0e38f) {
-        b->tune = best;
-        st = buildBatchedPlan(b);
+        st = buildBatchedPlan(b, best, b->precision);
         for (int k = 2; st == RP_OK && k <= max_steps_per_launch && k <= 8; k *= 2) {
             float ms = 0.0f;
             if ((st = snap.restore(b)) != RP_OK) break;
@@ -988,8 +1026,9 @@ rp_status rp_batch_autotune(rp_batch* b, const rp_step_params* p, int32_t max_st
         }
     }
     const rp_status trial = st;
-    b->tune = trial == RP_OK ? best : start;
-    st = buildBatchedPlan(b);
+    const Tune keep = trial == RP_OK ? best : start;
+    st = buildBatchedPlan(b, keep, b->precision);
+    if (st == RP_OK) b->tune = keep;
     const rp_status back = snap.restore(b);
     const rp_status sync = syncBatch(b);
     b->launches = launches0;

@@ -708,8 +708,14 @@ cudaError_t batchedReserveSmem(size_t bytes) {
     return e;
 }
 
-cudaError_t batchedOccupancy(int threads, size_t smem, int* perSm) {
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(perSm, kBatchedStep<false, false>, threads, smem);
+cudaError_t batchedOccupancy(int threads, size_t smem, int precision, int* perSm) {
+    // the instance the launch will use: register counts differ between them
+    const bool comp = (precision & 1) != 0, fp64 = (precision & 2) != 0;
+    if (comp)
+        return fp64 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(perSm, kBatchedStep<true, true>, threads, smem)
+                    : cudaOccupancyMaxActiveBlocksPerMultiprocessor(perSm, kBatchedStep<true, false>, threads, smem);
+    return fp64 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(perSm, kBatchedStep<false, true>, threads, smem)
+                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(perSm, kBatchedStep<false, false>, threads, smem);
 }
 
 }  // namespace rp

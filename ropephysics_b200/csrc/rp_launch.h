@@ -26,7 +26,7 @@ struct BatchedPlan {
 cudaError_t launchBatchedStep(const DArgs& a, const BatchedPlan& plan, int precision,
                               cudaStream_t stream);
 cudaError_t batchedReserveSmem(size_t bytes);
-cudaError_t batchedOccupancy(int threads, size_t smemBytes, int* blocksPerSm);
+cudaError_t batchedOccupancy(int threads, size_t smemBytes, int precision, int* blocksPerSm);
 
 // Address and size of this device's static scratch array (looked up on the
 // first call per device, with that device current).

@@ -320,7 +320,7 @@ bool rp_server::plan() {
         return false;
     }
     int perSm = 0;
-    if (rp::batchedOccupancy(256, smem, &perSm) != cudaSuccess || perSm < 1) {
+    if (rp::batchedOccupancy(256, smem, cfg.precision, &perSm) != cudaSuccess || perSm < 1) {
         cudaGetLastError();
         workerError = "batched kernel not resident";
         return false;

@@ -1,7 +1,9 @@
 """Seeded synthetic workloads with the shapes of the benchmark configurations.
 
 No external data: every rod, material draw, drive and primitive comes from a
-numpy Generator seeded by the caller.
+numpy Generator seeded by the caller. The uneven batch and the grid take their
+draws from ``synth`` (numpy only), which the CPU reference timing shares, so
+both sides simulate the same rods.
 
   cantilever   1 clamped rod, 64 segments, 1 m, r 5 mm, E 1e8, nu 0.3,
                rho 1100, gravity plus a 0.05 N tip load; dt 1/60, 20 substeps
@@ -27,8 +29,18 @@ from typing import List, Optional
 import numpy as np
 
 from . import Batch, Drive, Material, Primitive, Rod, StepParams, Strategy, World
+from . import synth
+from .synth import helix, table_for  # noqa: F401  (re-exported for callers)
 
-GRID_MATERIAL = Material(youngs=1e8, poisson=0.3, density=1100.0, radius=5e-3)
+GRID_MATERIAL = Material(youngs=synth.YOUNGS, poisson=synth.POISSON, density=synth.DENSITY,
+                         radius=synth.RADIUS)
+
+
+def primitive(spec) -> Primitive:
+    """A Primitive from a synth spec tuple."""
+    t, a, b, n, h, r, radius, mu = spec
+    return Primitive(int(t), a=tuple(a), b=tuple(b), normal=tuple(n), half_extents=tuple(h),
+                     rotation=tuple(r), radius=float(radius), friction=float(mu))
 
 
 @dataclass
@@ -75,95 +87,34 @@ def cantilever() -> Workload:
 
 def grid(num_rods: int = 4096, seed: int = 0) -> Workload:
     """Plain batched grid: hanging rods, per-rod stiffness/friction, driven tops."""
-    rng = np.random.default_rng(seed)
+    d = synth.grid(num_rods, seed)
     rod = Rod.straight(64, 1.0, GRID_MATERIAL, origin=(0.0, 0.0, 0.0), direction=(0.0, 0.0, -1.0))
     rod.pin_particle(0)
     world = World([Primitive.plane((0.0, 0.0, -1.2), (0.0, 0.0, 1.0), 0.5)])
-    ys = rng.uniform(0.4, 4.0, num_rods).astype(np.float32)
-    fs = rng.uniform(0.6, 1.4, num_rods).astype(np.float32)
-    amp = rng.uniform(0.0, 0.1, num_rods)
-    freq = rng.uniform(0.5, 2.0, num_rods)
-    phase = rng.uniform(0.0, 2 * math.pi, num_rods)
+    ys, fs = d.youngs_scale, d.friction_scale
     drives = [Drive(0, (0.0, 0.0, 1.0), float(a), float(f), float(p))
-              for a, f, p in zip(amp, freq, phase)]
+              for a, f, p in zip(d.amplitude, d.frequency, d.phase)]
     return Workload(f"grid-{num_rods}x64", [rod] * num_rods, [world], [0] * num_rods,
                     StepParams(dt=1.0 / 60, substeps=20, iterations=1), ys, fs, drives, steps=1000,
                     info=dict(seed=seed))
 
 
-def helix(n: int, length: float, coil_radius: float, pitch: float, origin=(0.0, 0.0, 0.0)):
-    """n+1 points of arc length `length` on a vertical helix."""
-    turn = math.sqrt((2 * math.pi * coil_radius) ** 2 + pitch ** 2)
-    total = 2 * math.pi * length / turn
-    t = np.linspace(0.0, total, n + 1)
-    o = np.asarray(origin, float)
-    return np.stack([o[0] + coil_radius * np.cos(t), o[1] + coil_radius * np.sin(t),
-                     o[2] + pitch * t / (2 * math.pi)], axis=1)
-
-
-def _random_quat(rng):
-    q = rng.normal(size=4)
-    return tuple(q / np.linalg.norm(q))
-
-
-def _random_primitive(rng, centre, mu, lo, hi, clearance=0.02, tries=64):
-    """A sphere, capsule or box centred within 1 m of `centre` whose bounding
-    sphere keeps `clearance` from the rod's box [lo, hi] (no rod starts inside
-    a primitive)."""
-    for _ in range(tries):
-        kind = int(rng.integers(1, 4))  # sphere, capsule, box
-        d = rng.normal(size=3)
-        d = d / np.linalg.norm(d) * rng.uniform(0.0, 1.0) ** (1.0 / 3.0)
-        c = np.asarray(centre) + d
-        if kind == 1:
-            r = float(rng.uniform(0.02, 0.2))
-            prim, bound = Primitive.sphere(tuple(c), r, mu), r
-        elif kind == 2:
-            axis = rng.normal(size=3)
-            half = rng.uniform(0.1, 0.5) * 0.5
-            axis = axis / np.linalg.norm(axis) * half
-            r = float(rng.uniform(0.01, 0.05))
-            prim = Primitive.capsule(tuple(c - axis), tuple(c + axis), r, mu)
-            bound = half + r
-        else:
-            h = rng.uniform(0.05, 0.3, 3)
-            prim, bound = Primitive.box(tuple(c), tuple(h), _random_quat(rng), mu), float(np.linalg.norm(h))
-        gap = np.linalg.norm(np.maximum(np.abs(c - (lo + hi) / 2) - (hi - lo) / 2, 0.0)) - bound
-        if gap >= clearance:
-            return prim
-    return prim
-
-
-def table_for(segments: int, lo: int = 64, hi: int = 1024) -> int:
-    """Spatial-hash table size for a rod: the power of two >= 2 x segments,
-    clamped to [lo, hi] (few bucket collisions, bounded shared memory)."""
-    t = lo
-    while t < 2 * segments and t < hi:
-        t *= 2
-    return t
+def _random_primitive(rng, centre, mu, lo, hi, clearance=0.02, tries=64) -> Primitive:
+    """synth.random_primitive as a Primitive."""
+    return primitive(synth.random_primitive(rng, centre, mu, lo, hi, clearance, tries))
 
 
 def uneven(num_rods: int = 16384, seed: int = 0, min_seg: int = 16, max_seg: int = 512,
            substeps: int = 50, hash_table_size: int = 0) -> Workload:
     """Uneven batch: rods of 16..512 segments, coiled, each with its own world.
     hash_table_size 0 sizes each rod's table with table_for()."""
-    rng = np.random.default_rng(seed)
     rods, worlds = [], []
-    for _ in range(num_rods):
-        n = int(rng.integers(min_seg, max_seg + 1))
-        length = 0.2 * n / 32.0
-        rc = float(rng.uniform(0.05, 0.2))
-        pts = helix(n, length, rc, pitch=4.0 * GRID_MATERIAL.radius,
-                    origin=(0.0, 0.0, 0.0))
-        rod = Rod.centerline(pts, GRID_MATERIAL, frame_seed=(0.0, 0.0, 1.0))
+    for d in synth.uneven(num_rods, seed, min_seg, max_seg, hash_table_size):
+        rod = Rod.centerline(d.points, GRID_MATERIAL, frame_seed=(0.0, 0.0, 1.0))
         rod.b_rest_darboux[:] = 0.0  # straight rest shape: the coil is loaded
         rods.append(rod)
-        mu = float(rng.uniform(0.2, 1.0))
-        centre = pts.mean(axis=0)
-        lo, hi = pts.min(axis=0), pts.max(axis=0)
-        prims = [_random_primitive(rng, centre, mu, lo, hi) for _ in range(int(rng.integers(1, 5)))]
-        worlds.append(World(prims, self_collision=True, self_friction=mu,
-                            hash_table_size=hash_table_size or table_for(n)))
+        worlds.append(World([primitive(q) for q in d.prims], self_collision=True, self_friction=d.friction,
+                            hash_table_size=d.hash_table_size))
     return Workload(f"uneven-{num_rods}x[{min_seg},{max_seg}]", rods, worlds, list(range(num_rods)),
                     StepParams(dt=1.0 / 60, substeps=substeps, iterations=1), steps=500,
                     info=dict(seed=seed, hash_table_size=hash_table_size or "2n, pow2, 64..1024"))

@@ -17,8 +17,9 @@ own validation setups, and writes small fixtures that travel with the repo:
                      (rope pre-stepped until it holds >= 5 self contacts), its
                      contact list, and the state one step later.
 
-Usage: python tests/golden/make_golden.py   (needs /root/reference built into
-oracle/_ref; the fixtures are committed, so the tests do not.)
+Usage: python tests/golden/make_golden.py   (needs the reference's sources --
+$RP_REFERENCE, else a checkout beside the repository -- built into oracle/_ref
+by ``make -C oracle ref``; the fixtures are committed, so the tests do not.)
 """
 from __future__ import annotations
 

@@ -10,6 +10,8 @@
   FP64 oracle.
 * A world with 64 primitives (the maximum) steps identically under every
   strategy.
+* A precision change whose layout no longer fits is refused and leaves the
+  batch's plan untouched.
 """
 import numpy as np
 import pytest
@@ -82,3 +84,29 @@ def test_sixty_four_primitives():
     for s in STRATS:
         assert np.array_equal(res[s][0], ref[0]), s
     assert np.all(np.isfinite(ref[0]))
+
+
+def test_refused_precision_change_keeps_the_plan(oracle64):
+    """A clamped rod of 1700 segments fits the batched kernel's shared memory
+    in reference precision (lean layout 128 n + 416 bytes = 218 KB) but not
+    compensated (144 n + 432 bytes = 245 KB > 227 KB). Switching it to
+    compensated precision must fail with RP_ERR_SHARED_MEMORY and leave the
+    batch's plan as it was: same shared memory per CTA, and steps bitwise
+    equal to a batch that never tried."""
+    n = 1700
+    o = oracle64.straight(n, 1.7, youngs=1e8, poisson=0.3, density=1100.0, radius=5e-3)
+    oracle64.clamp(o, False)
+    proto = product_rod(o)
+    b = rp.Batch.create(proto, 2, rp.Strategy.BATCHED)
+    smem = b.shared_bytes_per_block
+    with pytest.raises(rp.RopeError) as e:
+        b.set_precision(int(rp.Precision.COMPENSATED))
+    assert e.value.status == 3 and "shared memory" in str(e.value)
+    assert b.shared_bytes_per_block == smem
+    b.step_many(P, 3)
+    fresh = rp.Batch.create(proto, 2, rp.Strategy.BATCHED)
+    fresh.step_many(P, 3)
+    assert np.array_equal(b.download_positions(), fresh.download_positions())
+    assert np.array_equal(b.download_frames(), fresh.download_frames())
+    b.close()
+    fresh.close()

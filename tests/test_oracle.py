@@ -18,6 +18,9 @@ from oracle import Context, Params, Primitive, World
 from tests.helpers import REF_MAT, benchmark_rod
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+# the reference's source tree: $RP_REFERENCE, else a checkout beside the repo
+REFERENCE = os.environ.get("RP_REFERENCE", os.path.join(os.path.dirname(os.path.dirname(
+    os.path.dirname(os.path.abspath(__file__)))), "reference"))
 
 
 def _fmt(v):
@@ -39,7 +42,7 @@ def test_crosscheck_golden_byte_exact(oracle64):
 
 def test_golden_matches_published_reference_data():
     """The fixture equals the reference's own docs/data/crosscheck.csv."""
-    pub = "/root/reference/docs/data/crosscheck.csv"
+    pub = os.path.join(REFERENCE, "docs", "data", "crosscheck.csv")
     if not os.path.exists(pub):
         pytest.skip("reference tree not present")
     assert open(pub).read().split() == open(os.path.join(GOLDEN, "crosscheck.csv")).read().split()
@@ -213,7 +216,8 @@ def test_op_count_oracle_reproduces_double():
 def test_flops_per_segment_substep_match_bench():
     """The bench's algorithmic FLOPs per segment-substep (add, sub, mul, div,
     sqrt) are the op-counting oracle's count for a pinned 64-segment rod at
-    dt 1/60 with 20 substeps, free and with a floor plane."""
+    dt 1/60 with 20 substeps, free (the cantilever) and with a floor plane
+    (the grid)."""
     import bench
     from oracle import Context, Oracle, Primitive as OP, World as OW
     oc = Oracle("count")
@@ -230,6 +234,65 @@ def test_flops_per_segment_substep_match_bench():
         return sum(c[k] for k in ("add", "mul", "div", "sqrt")) / (64 * 20)
 
     # the bench quotes them to one decimal
-    assert per_seg_substep(None) == pytest.approx(bench.FLOPS_PER_SEG_SUBSTEP["uneven"], abs=0.05)
+    assert per_seg_substep(None) == pytest.approx(bench.FLOPS_PER_SEG_SUBSTEP["cantilever"], abs=0.05)
     floor = OW([OP.plane((0, 0, -1.2), (0, 0, 1), 0.5)])
     assert per_seg_substep(floor) == pytest.approx(bench.FLOPS_PER_SEG_SUBSTEP["grid"], abs=0.05)
+
+
+def _counted_window(oc, rods, params, skip, count):
+    """FLOPs per segment-substep of `count` steps after `skip` steps of the
+    (rod, world, context, segments) tuples."""
+    for r, w, ctx, _ in rods:
+        oc.step(r, params, world=w, ctx=ctx, steps=skip)
+    oc.op_reset()
+    for r, w, ctx, _ in rods:
+        oc.step(r, params, world=w, ctx=ctx, steps=count)
+    c = oc.op_counts()
+    segs = sum(s for *_, s in rods)
+    return sum(c[k] for k in ("add", "mul", "div", "sqrt")) / (segs * params.substeps * count)
+
+
+def test_flops_per_segment_substep_uneven_batch():
+    """The uneven batch's count includes its contacts and self-collision:
+    32 rods sampled as the bench's CPU leg samples them (seed 123) from the
+    seed-0 draws, built by the oracle's builders, counted over steps 25-44."""
+    import bench
+    from oracle import Context, Oracle, Primitive as OP, World as OW
+    from ropephysics_b200 import synth
+    oc = Oracle("count")
+    draws = synth.uneven(16384, 0)
+    idx = np.random.default_rng(123).choice(len(draws), size=32, replace=False)
+    f32 = lambda v: float(np.float32(v))
+    p = Params(dt=f32(1 / 60), substeps=50, iterations=1, gravity=(0.0, 0.0, f32(-9.81)))
+    rods = []
+    for i in idx:
+        d = draws[i]
+        r = oc.centerline(d.points, youngs=synth.YOUNGS, poisson=synth.POISSON, density=synth.DENSITY,
+                          radius=synth.RADIUS, frame_seed=(0, 0, 1))
+        r.bRestD[:] = 0.0
+        w = OW([OP(*q) for q in d.prims], True, d.friction, 2, d.hash_table_size, 0.25)
+        rods.append((r, w, Context(dtype=np.float64), d.segments))
+    assert _counted_window(oc, rods, p, 25, 20) == pytest.approx(bench.FLOPS_PER_SEG_SUBSTEP["uneven"],
+                                                                 abs=0.05)
+
+
+def test_flops_per_segment_substep_hook_sweep():
+    """The hook sweep's count: 16 placements spread over the sweep (leg ratio,
+    friction, stiffness), on the bar and floor with self-collision, counted
+    over steps 23-42 (the window the bench's shape timing measures)."""
+    import bench
+    from oracle import Context, Oracle, Primitive as OP, World as OW
+    from ropephysics_b200 import workloads as W
+    oc = Oracle("count")
+    f32 = lambda v: float(np.float32(v))
+    p = Params(dt=f32(1 / 60), substeps=20, iterations=1, gravity=(0.0, 0.0, f32(-9.81)))
+    rods = []
+    for k in range(16):
+        ratio, mu, youngs = 1.0 + 3.0 * k / 15, 0.05 + 0.55 * ((7 * k) % 16) / 15, (1e8, 3e8)[k % 2]
+        r = oc.centerline(W.hanging_cable_points(ratio), youngs=youngs, frame_seed=(0, 1, 0),
+                          **W.HOOK_MATERIAL)
+        r.bRestD[:] = 0.0
+        w = OW([OP.capsule((0.0, -0.3, 0.8), (0.0, 0.3, 0.8), 0.02, mu), OP.plane((0, 0, 0), (0, 0, 1), mu)],
+               True, mu, 2, 256, 0.25)
+        rods.append((r, w, Context(dtype=np.float64), 120))
+    assert _counted_window(oc, rods, p, 23, 20) == pytest.approx(bench.FLOPS_PER_SEG_SUBSTEP["hook"], abs=0.05)
