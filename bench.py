@@ -148,10 +148,10 @@ def barrier(world: int):
         dist.barrier()
 
 
-def build_workload(name: str, rods: int, seed: int):
+def build_workload(name: str, rods: int, seed: int, shard=None):
     from ropephysics_b200 import workloads
     if name == "uneven":
-        return workloads.uneven(rods or 16384, seed=seed)
+        return workloads.uneven(rods or 16384, seed=seed, shard=shard)
     if name == "grid":
         return workloads.grid(rods or 4096, seed=seed)
     if name == "cantilever":
@@ -475,10 +475,14 @@ def run_ours(args):
     torch.cuda.set_device(local)
     import ropephysics_b200 as rp
 
-    wl = build_workload(args.workload, args.rods, seed=args.seed + rank)
-    config = workload_config(args.workload, args.rods, args.seed + rank)
-    config["parallelism"] = f"replicas{world_size}"
-    assert config["segments"] == int(wl.segments.sum()) and config["workload"] == wl.name
+    # N ranks: shards of one seeded batch of N x rods (every rank the same
+    # spread of lengths; weak scaling), else independent replicas
+    shard = (rank, world_size) if world_size > 1 and args.workload == "uneven" else None
+    wl = build_workload(args.workload, args.rods, seed=args.seed if shard else args.seed + rank, shard=shard)
+    config = workload_config(args.workload, args.rods, args.seed)
+    config["parallelism"] = f"shards{world_size}" if shard else f"replicas{world_size}"
+    if world_size == 1:
+        assert config["segments"] == int(wl.segments.sum()) and config["workload"] == wl.name
     seg_sub = wl.segment_substeps_per_step()
     p = wl.params
     # the roofline denominator, measured on this device before anything else runs
@@ -643,6 +647,111 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def reference_gpu_rates(seed: int) -> dict:
+    """The reference's own FP32 GPU batch (src/gpu/gpu_solver.cu and
+    gpu_batch.cpp, built for sm_100a into oracle/_ref/libcrs_ref_gpu.so) on
+    the shapes its API can express, driven the way its API drives them:
+    one Batch::step per step, kinematic velocities uploaded from the host
+    every step, wall time over the steps with a device synchronise at the
+    end (the reference's calls are synchronous).
+      grid              the 4096 x 64 driven grid in full: one fused batch,
+                        per-rod stiffness and friction scales, floor
+      uneven_by_length  the uneven batch grouped by length (its Batch holds
+                        one prototype and one world): 8 lengths spread over
+                        16..512, every rod of that length as one batch with
+                        self-collision on and no primitives; fused where its
+                        shared memory allows, else its multi-kernel path"""
+    import oracle as orc
+    S = load_synth()
+    try:
+        R = orc.Reference(gpu=True)
+    except Exception as e:  # the reference GPU build is absent
+        return {"unavailable": f"reference GPU library: {e}"}
+    if not R.lib.refgpu_available():
+        return {"unavailable": "no CUDA device"}
+    FP = C.POINTER(C.c_float)
+    mat = dict(youngs=S.YOUNGS, poisson=S.POISSON, density=S.DENSITY, radius=S.RADIUS)
+    out = {"unit": "segment-substeps/s", "timing": "wall clock, synchronised, reference API call pattern"}
+    # ---- grid ----
+    dt, sub = WORKLOAD_PARAMS["grid"]
+    g = S.grid(4096, seed)
+    h = R.straight(64, 1.0, origin=(0.0, 0.0, 0.0), direction=(0.0, 0.0, -1.0), **mat)
+    rr = R.export(h)
+    rr.invMass[0] = 0.0
+    R.import_state(h, rr)
+    wh = R.world(orc.World([orc.Primitive(*S.plane((0.0, 0.0, -1.2), (0.0, 0.0, 1.0), 0.5))]))
+    rb = R.lib.refgpu_create(h, 4096, 1, wh)
+    grav = (C.c_double * 3)(0.0, 0.0, float(np.float32(-9.81)))
+    ys = np.ascontiguousarray(g.youngs_scale, np.float32)
+    fs = np.ascontiguousarray(g.friction_scale, np.float32)
+    R.lib.refgpu_set_material_scales(rb, ys.ctypes.data_as(FP), fs.ctypes.data_as(FP), 4096)
+    kin = np.zeros((4096, 65, 3), np.float32)
+    w = 2 * math.pi * g.frequency
+
+    def grid_step(s):
+        kin[:, 0, 2] = g.amplitude * w * np.cos(w * s * dt + g.phase)
+        R.lib.refgpu_set_kinematic(rb, kin.ctypes.data_as(FP), 4096 * 65)
+        R.lib.refgpu_step(rb, dt, sub, 1, grav, 0.0, 0.0, 1, 1)
+
+    for s in range(3):
+        grid_step(s)
+    R.lib.refgpu_sync(rb)
+    steps = 20
+    t0 = time.perf_counter()
+    for s in range(steps):
+        grid_step(3 + s)
+    R.lib.refgpu_sync(rb)
+    t = time.perf_counter() - t0
+    out["grid"] = {"workload": "grid-4096x64", "rate": 4096 * 64 * sub * steps / t,
+                   "ms_per_step": t * 1e3 / steps, "strategy": "fused"}
+    R.lib.refgpu_free(rb)
+    R.free(h)
+    # ---- uneven batch, grouped by length ----
+    dt, sub = WORKLOAD_PARAMS["uneven"]
+    draws = S.uneven(16384, seed)
+    by_len = {}
+    for d in draws:
+        by_len.setdefault(d.segments, []).append(d)
+    lengths = sorted(by_len)
+    pick = [lengths[int(round(i * (len(lengths) - 1) / 7))] for i in range(8)]
+    total_work, total_t, groups = 0, 0.0, []
+    for n in pick:
+        rods = by_len[n]
+        hs = []
+        for d in rods:
+            hh = R.centerline(d.points, frame_seed=(0.0, 0.0, 1.0), **mat)
+            q = R.export(hh)
+            q.bRestD[:] = 0.0
+            R.import_state(hh, q)
+            hs.append(hh)
+        wh = R.world(orc.World([], True, rods[0].friction, 2, rods[0].hash_table_size, 0.25))
+        fused = 1
+        rb = R.lib.refgpu_create(hs[0], len(hs), 1, wh)
+        if not rb:
+            fused = 0
+            rb = R.lib.refgpu_create(hs[0], len(hs), 0, wh)
+        for i, hh in enumerate(hs):
+            R.lib.refgpu_upload_rod(rb, i, hh)
+        R.lib.refgpu_step(rb, dt, sub, 1, grav, 0.0, 0.0, 1, 1)
+        R.lib.refgpu_sync(rb)
+        k = 3
+        t0 = time.perf_counter()
+        R.lib.refgpu_step(rb, dt, sub, 1, grav, 0.0, 0.0, 1, k)
+        R.lib.refgpu_sync(rb)
+        t = time.perf_counter() - t0
+        total_work += len(hs) * n * sub * k
+        total_t += t
+        groups.append({"segments": n, "rods": len(hs), "strategy": "fused" if fused else "multi-kernel",
+                       "ms_per_step": t * 1e3 / k})
+        R.lib.refgpu_free(rb)
+        for hh in hs:
+            R.free(hh)
+    out["uneven_by_length"] = {"rate": total_work / total_t, "groups": groups,
+                               "sample": "8 lengths over 16..512, every rod of each length, self-collision, "
+                                         "no primitives, 3 steps each"}
+    return out
+
+
 def run_reference(args):
     """The reference's own FP64 CPU step on this box's host cores, on the
     workload's seeded draws: this process never imports ropephysics_b200.
@@ -677,6 +786,8 @@ def run_reference(args):
                              "kind": "reference", "sample": desc},
             "e2e": {"value": value, "unit": "segment-substeps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
+    if not args.no_reference_gpu:
+        line["reference_gpu"] = reference_gpu_rates(args.seed)
     print(json.dumps(line), flush=True)
 
 
@@ -694,6 +805,7 @@ def main():
     ap.add_argument("--no-shapes", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true")
     ap.add_argument("--cpu-rods", type=int, default=256)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-served", action="store_true")

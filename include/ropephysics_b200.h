@@ -355,9 +355,12 @@ rp_status rp_batch_set_graph(rp_batch* batch, int32_t enabled);
  * CTA = CTA size / team size), pairs per thread (a rod of n segments gets a
  * team of about n / (2 x pairs) threads, whole warps, 32..256) and whole steps
  * per launch in rp_batch_step_many. None of them changes results.
+ * cta_threads 0 selects one rod per CTA with every array staged in shared
+ * memory (the RP_STRATEGY_FUSED kernel, same results), which wins for a few
+ * short rods; it needs each rod's full layout to fit one CTA.
  * rp_batch_autotune times the candidate shapes on this batch with its current
  * state (restored afterwards) and keeps the fastest; steps per launch is
- * tried up to max_steps_per_launch (at most 8). */
+ * tried up to max_steps_per_launch (at most 8), then one rod per CTA. */
 rp_status rp_batch_autotune(rp_batch* batch, const rp_step_params* params, int32_t max_steps_per_launch);
 rp_status rp_batch_get_tuning(const rp_batch* batch, int32_t* cta_threads, int32_t* pairs_per_thread,
                               int32_t* steps_per_launch);
@@ -432,6 +435,13 @@ rp_status rp_batch_read_self_contacts(rp_batch* batch, int32_t rod, int32_t* pai
  * arming time; held = max rise <= tolerance. particle < 0 disarms. */
 rp_status rp_batch_arm_hold_observer(rp_batch* batch, const int32_t* particle_of_rod,
                                      int32_t n, int32_t interval, double tolerance);
+/* The same, with each rod's start height given by the caller (start_z, one
+ * per rod; NULL = read from the device as above). The reference's outcome
+ * starts from the host rod's double height (HangOutcome(rod.state.x.front().z),
+ * application_cases.cpp:47-50), not from its float copy on the device. */
+rp_status rp_batch_arm_hold_observer_at(rp_batch* batch, const int32_t* particle_of_rod,
+                                        const double* start_z, int32_t n, int32_t interval,
+                                        double tolerance);
 /* max_rise (may be NULL) and held (may be NULL), one per rod; near_boundary
  * (may be NULL) flags rods whose max rise lies within float resolution of the
  * tolerance, classified in FP64 when RP_PRECISION_FP64_VERDICT is set. */

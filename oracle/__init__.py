@@ -477,6 +477,8 @@ class Reference:
             L.refgpu_overflow.argtypes = [vp]
             L.refgpu_self_pairs.argtypes = [vp, C.c_int, C.POINTER(C.c_int), C.c_int]
             L.refgpu_contact_active.argtypes = [vp, C.c_int, C.POINTER(C.c_int)]
+            fp = C.POINTER(C.c_float)
+            L.refgpu_download_state.argtypes = [vp, fp, fp, fp, fp]
 
     # ---- the harness-routing task (src/apps/harness_routing.h:27-97) ----
     @staticmethod
@@ -526,6 +528,18 @@ class Reference:
         n = self.lib.refgpu_self_pairs(batch, rod, out.ctypes.data_as(C.POINTER(C.c_int)), cap)
         assert n >= 0, "reference batch is not multi-kernel or has no self-collision"
         return [tuple(int(v) for v in p) for p in out[:n]]
+
+    def gpu_state(self, batch, num_rods, num_particles, num_frames):
+        """(x, v, q, omega) of every rod of a reference GPU batch, float32,
+        shaped (rods, particles, 3) and (rods, frames, 4 | 3)."""
+        x = np.zeros((num_rods, num_particles, 3), np.float32)
+        v = np.zeros_like(x)
+        q = np.zeros((num_rods, num_frames, 4), np.float32)
+        w = np.zeros((num_rods, num_frames, 3), np.float32)
+        fp = C.POINTER(C.c_float)
+        self.lib.refgpu_download_state(batch, x.ctypes.data_as(fp), v.ctypes.data_as(fp), q.ctypes.data_as(fp),
+                                       w.ctypes.data_as(fp))
+        return x, v, q, w
 
     def gpu_contact_active(self, batch, rod, num_particles, num_prims):
         out = np.zeros(num_particles * num_prims, np.int32)

@@ -514,6 +514,36 @@ int refgpu_contact_active(void* bp, int rod, int* active) {
         for (int k = 0; k < np; ++k) active[i * np + k] = all[(std::size_t(i) * R + rod) * np + k].active;
     return nP * np;
 }
+// The whole batch's state, one device copy per array, rod-major: x and v
+// (3 floats per particle), q (w, x, y, z per frame) and omega (3 per frame).
+// Batch::download copies every array once per rod (gpu_batch.cpp:393-416),
+// which is too slow for restart comparisons of thousands of rods.
+int refgpu_download_state(void* bp, float* x, float* v, float* q, float* w) {
+    auto* b = static_cast<gpu::Batch*>(bp);
+    const gpu::DevRodF& d = b->impl_->rod;
+    const gpu::DevStateF& st = b->impl_->state;
+    const std::size_t nP = d.numParticles, nS = d.numSegments, R = d.numRods;
+    const bool rodMajor = b->strategy_ == gpu::Strategy::kFused;
+    std::vector<Vec3f> hx(nP * R), hv(nP * R), hw(nS * R);
+    std::vector<Quatf> hq(nS * R);
+    gpu::copyToHost(hx.data(), st.x, hx.size() * sizeof(Vec3f));
+    gpu::copyToHost(hv.data(), st.v, hv.size() * sizeof(Vec3f));
+    gpu::copyToHost(hq.data(), st.q, hq.size() * sizeof(Quatf));
+    gpu::copyToHost(hw.data(), st.omega, hw.size() * sizeof(Vec3f));
+    for (std::size_t r = 0; r < R; ++r) {
+        for (std::size_t i = 0; i < nP; ++i) {
+            const std::size_t at = rodMajor ? r * nP + i : i * R + r, o = 3 * (r * nP + i);
+            x[o] = hx[at].x, x[o + 1] = hx[at].y, x[o + 2] = hx[at].z;
+            v[o] = hv[at].x, v[o + 1] = hv[at].y, v[o + 2] = hv[at].z;
+        }
+        for (std::size_t j = 0; j < nS; ++j) {
+            const std::size_t at = rodMajor ? r * nS + j : j * R + r, o = r * nS + j;
+            q[4 * o] = hq[at].w, q[4 * o + 1] = hq[at].x, q[4 * o + 2] = hq[at].y, q[4 * o + 3] = hq[at].z;
+            w[3 * o] = hw[at].x, w[3 * o + 1] = hw[at].y, w[3 * o + 2] = hw[at].z;
+        }
+    }
+    return int(R);
+}
 int refgpu_available() { return gpu::cudaAvailable() ? 1 : 0; }
 #endif
 

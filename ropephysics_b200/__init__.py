@@ -629,10 +629,19 @@ class Batch:
                                                  out.shape[0], C.byref(n)))
         return out[: n.value]
 
-    def arm_hold_observer(self, particle_of_rod, interval: int = 50, tolerance: float = 0.05):
+    def arm_hold_observer(self, particle_of_rod, interval: int = 50, tolerance: float = 0.05, start_z=None):
+        """start_z: each rod's start height (e.g. the double the rod was built
+        from); None reads it from the device."""
         p = np.ascontiguousarray(particle_of_rod, np.int32)
-        _check(lib().rp_batch_arm_hold_observer(self._h, p.ctypes.data_as(_I32), len(p), interval,
-                                                tolerance))
+        if start_z is None:
+            _check(lib().rp_batch_arm_hold_observer(self._h, p.ctypes.data_as(_I32), len(p), interval,
+                                                    tolerance))
+            return
+        z = np.ascontiguousarray(start_z, np.float64)
+        if len(z) != len(p):
+            raise ValueError("start_z needs one height per rod")
+        _check(lib().rp_batch_arm_hold_observer_at(self._h, p.ctypes.data_as(_I32), z.ctypes.data_as(_F64),
+                                                   len(p), interval, tolerance))
 
     def read_hold_verdicts(self):
         n = self.num_rods

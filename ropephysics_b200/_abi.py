@@ -154,6 +154,7 @@ SIGNATURES = {
     "rp_batch_read_contact_states": (i32, [vp, P(u8), i64, P(i64)]),
     "rp_batch_read_self_contacts": (i32, [vp, i32, P(i32), i32, P(i32)]),
     "rp_batch_arm_hold_observer": (i32, [vp, P(i32), i32, i32, f64]),
+    "rp_batch_arm_hold_observer_at": (i32, [vp, P(i32), P(f64), i32, i32, f64]),
     "rp_batch_read_hold_verdicts": (i32, [vp, P(f64), P(u8), P(u8), i32]),
     "rp_batch_num_rods": (i32, [vp]),
     "rp_batch_num_segments": (i32, [vp, i32]),

@@ -30,9 +30,10 @@ CXX_FLAGS = ["-std=c++17", "-O3", "-fPIC", "-Wall", "-Wextra", "-Wno-unused-para
 
 CU_SOURCES = ["rp_plain.cu", "rp_batched.cu", "rp_static_scratch.cu", "rp_traj.cu", "rp_harness.cu",
               "rp_peak.cu"]
-CPP_SOURCES = ["rp_rod.cpp", "rp_hostutil.cpp", "rp_batch.cpp", "rp_server.cpp", "rp_traj.cpp"]
+CPP_SOURCES = ["rp_rod.cpp", "rp_hostutil.cpp", "rp_batch.cpp", "rp_batch_tune.cpp", "rp_batch_io.cpp",
+               "rp_server.cpp", "rp_traj.cpp"]
 HEADERS = ["rp_internal.h", "rp_layout.h", "rp_launch.h", "rp_math.cuh", "rp_step_common.cuh",
-           "rp_host.h"]
+           "rp_host.h", "rp_batch_impl.h", "rp_bulk.cuh"]
 
 
 def _newest_dep() -> float:

@@ -22,6 +22,7 @@
 #include "rp_internal.h"
 #include "rp_launch.h"
 #include "rp_layout.h"
+#include "rp_batch_impl.h"
 
 using rp::DArgs;
 using rp::DPrim;
@@ -41,110 +42,9 @@ rp_status fail(rp_status s, const std::string& msg) {
 
 using rpx::fail;
 
-#define RP_CUDA(call)                                                                     \
-    do {                                                                                  \
-        cudaError_t e_ = (call);                                                          \
-        if (e_ != cudaSuccess)                                                            \
-            return fail(RP_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
-    } while (0)
 
-namespace {
 
-// Launch choices for the batched form, picked by rp_batch_autotune.
-struct Tune {
-    int ctaThreads = 256;     // threads per CTA (rods per CTA = ctaThreads / team)
-    int pairsPerThread = 1;   // team threads ~ ceil(nSt / 2 / pairsPerThread), rounded to 32
-    int stepsPerLaunch = 1;   // whole steps (x substeps) per launch in rp_batch_step_many
-};
-
-}  // namespace
-
-struct rp_batch {
-    int device = 0;
-    rp_strategy strategy = RP_STRATEGY_FUSED;
-    int numRods = 0;
-    int precision = 0;
-    cudaStream_t stream = nullptr;
-    bool ownStream = false;
-    int plainThreads = 128;
-    size_t smemBytes = 0;
-    int maxPrims = 0;
-    bool anySelf = false;
-    int sColorsMax = 0, bColorsMax = 0;
-    long long launches = 0;
-
-    std::vector<DTemplate> tmpls;
-    std::vector<DRod> rods;
-    std::vector<int> tmplNP;        // per rod particles (host copy)
-    std::vector<int> tmplNS;        // per rod frames
-    std::vector<std::vector<char>> fixedFrame;  // per template: frame is fixed (zero inertia)
-    int64_t totalP = 0, totalS = 0, totalSt = 0, totalB = 0, totalSlots = 0;
-    int64_t totalPool = 0, totalHash = 0;
-
-    std::vector<void*> owned;
-    DArgs a{};
-    rp::DDrive* driveStore = nullptr;          // sinusoidal drives, kept while waypoints are in use
-    rp::DWaypoints* waypointStore = nullptr;   // waypoint schedules, kept while drives are in use
-    rp::DOutcome* outcomes = nullptr;          // harness evaluation output
-    int32_t* dWork = nullptr;
-
-    // batched plan
-    std::vector<int32_t> groups;  // 4 ints per group
-    int32_t* dGroups = nullptr;
-    int32_t* dQueue = nullptr;
-    int numGroups = 0;
-    int batchedBlocks = 0;
-    int batchedThreads = 256;
-    size_t batchedSmem = 0;
-    Tune tune;
-
-    // graphs
-    bool useGraph = false;
-    cudaGraphExec_t graphExec = nullptr;
-    int graphSteps = 0;
-    int graphStepsPerLaunch = 0;
-    long long graphLaunches = 0;  // kernel launches in the captured graph
-    rp_step_params graphParams{};
-    int graphPrecision = -1;
-
-    // hold observer
-    int holdInterval = 0;
-    double holdTolerance = 0.05;
-    bool holdArmed = false;
-
-    ~rp_batch() {
-        if (graphExec) cudaGraphExecDestroy(graphExec);
-        for (void* p : owned) cudaFree(p);
-        if (ownStream && stream) cudaStreamDestroy(stream);
-    }
-
-    template <typename T>
-    rp_status alloc(T*& out, size_t count, bool zero = true) {
-        out = nullptr;
-        if (count == 0) count = 1;
-        void* p = nullptr;
-        const cudaError_t e = cudaMalloc(&p, count * sizeof(T));
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            return fail(RP_ERR_OUT_OF_MEMORY, "cudaMalloc of " + std::to_string(count * sizeof(T)) +
-                                                  " bytes failed: " + cudaGetErrorString(e));
-        }
-        owned.push_back(p);
-        if (zero) {
-            const cudaError_t z = cudaMemsetAsync(p, 0, count * sizeof(T), stream);
-            if (z != cudaSuccess) return fail(RP_ERR_CUDA, cudaGetErrorString(z));
-        }
-        out = static_cast<T*>(p);
-        return RP_OK;
-    }
-
-    template <typename T>
-    rp_status upload(T* dst, const std::vector<T>& src) {
-        if (src.empty()) return RP_OK;
-        RP_CUDA(cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
-        return RP_OK;
-    }
-};
+using rpx::Tune;
 
 namespace {
 
@@ -155,12 +55,6 @@ using rpx::packFrames;
 using rpx::packParticles;
 using rpx::toDPrim;
 using rpx::validateWorld;
-
-bool sameTopology(const rp_batch* b, int r, const rp_rod_desc* d) {
-    return d && d->num_particles == b->tmplNP[r] && d->num_frames == b->tmplNS[r];
-}
-
-rp_status buildBatchedPlan(rp_batch* b, const Tune& tune, int precision);
 
 }  // namespace
 
@@ -457,7 +351,7 @@ static rp_status createImpl(const rp_rod_desc* const* rods, int numRods, const r
 
 // ---------------------------------------------------------------- batched plan
 
-namespace {
+namespace rpx {
 
 // Plans the batched launch for `tune` and `precision` and commits it only
 // when every step succeeded: on failure the batch keeps its previous plan,
@@ -471,6 +365,7 @@ rp_status buildBatchedPlan(rp_batch* b, const Tune& tune, int precision) {
     const int cta = tune.ctaThreads;
     const bool comp = (precision & RP_PRECISION_COMPENSATED) != 0;
     const size_t optin = optinSmem(b->device);
+    const size_t fixed = rp::batchedStaticSmem() + 64;  // the kernel's own shared memory
     // World contact slots go into shared memory when the groups still fit as
     // many CTAs per SM with them (few contact primitives per rod, or short
     // rods); otherwise they stay in global memory.
@@ -482,7 +377,7 @@ rp_status buildBatchedPlan(rp_batch* b, const Tune& tune, int precision) {
         const size_t smem2 = rpx::planGroups(ids, b->rods.data(), b->tmpls.data(), cta, tune.pairsPerThread,
                                              comp, order2, groups2, true);
         int per1 = 0, per2 = 0;
-        if (smem2 + 1024 <= optin && rp::batchedReserveSmem(std::max(smem2, maxSmem)) == cudaSuccess &&
+        if (smem2 + fixed <= optin && rp::batchedReserveSmem(std::max(smem2, maxSmem)) == cudaSuccess &&
             rp::batchedOccupancy(cta, maxSmem, precision, &per1) == cudaSuccess &&
             rp::batchedOccupancy(cta, smem2, precision, &per2) == cudaSuccess && per2 >= per1 && per2 >= 1) {
             maxSmem = smem2;
@@ -492,7 +387,7 @@ rp_status buildBatchedPlan(rp_batch* b, const Tune& tune, int precision) {
         }
         cudaGetLastError();
     }
-    if (maxSmem + 1024 > optin)  // the kernel also has a few bytes of static shared memory
+    if (maxSmem + fixed > optin)
         return fail(RP_ERR_SHARED_MEMORY, "a rod group needs " + std::to_string(maxSmem) +
                                               " bytes of shared memory; the device allows " +
                                               std::to_string(optin));
@@ -561,11 +456,11 @@ rp_status buildBatchedPlan(rp_batch* b, const Tune& tune, int precision) {
     return RP_OK;
 }
 
-}  // namespace
+}  // namespace rpx
 
 // ---------------------------------------------------------------- stepping
 
-namespace {
+namespace rpx {
 
 void fillStepArgs(rp_batch* b, const rp_step_params* p, DArgs& A) {
     A.h = p->dt / p->substeps;
@@ -592,12 +487,12 @@ rp_status validateParams(const rp_step_params* p) {
 
 // One launch of `steps` whole steps (more than one only for the batched
 // strategy, whose kernel keeps each rod on chip across them).
-rp_status launchStep(rp_batch* b, const rp_step_params* p, int steps = 1) {
+rp_status launchStep(rp_batch* b, const rp_step_params* p, int steps) {
     DArgs A = b->a;
     fillStepArgs(b, p, A);
     A.stepsPerLaunch = steps;
     cudaError_t e;
-    if (b->strategy == RP_STRATEGY_BATCHED) {
+    if (b->strategy == RP_STRATEGY_BATCHED && !b->tune.plain) {
         rp::BatchedPlan plan;
         plan.groups = b->dGroups;
         plan.numGroups = b->numGroups;
@@ -623,7 +518,27 @@ rp_status syncBatch(rp_batch* b) {
     return RP_OK;
 }
 
-}  // namespace
+// Can the plain kernel step this batch (every rod's full layout in one
+// CTA's shared memory)? Opts the kernel into that much if so.
+rp_status reservePlain(rp_batch* b) {
+    if (b->smemBytes + 1024 > optinSmem(b->device))
+        return fail(RP_ERR_SHARED_MEMORY, "a rod needs " + std::to_string(b->smemBytes) +
+                                              " bytes of shared memory to run one rod per CTA");
+    if (rp::plainReserveSmem(std::max<size_t>(b->smemBytes, 1)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(RP_ERR_SHARED_MEMORY, "cannot opt into the shared memory one rod per CTA needs");
+    }
+    return RP_OK;
+}
+
+}  // namespace rpx
+
+using rpx::buildBatchedPlan;
+using rpx::fillStepArgs;
+using rpx::launchStep;
+using rpx::reservePlain;
+using rpx::syncBatch;
+using rpx::validateParams;
 
 // ---------------------------------------------------------------- C ABI
 
@@ -776,7 +691,8 @@ rp_status rp_batch_step_many(rp_batch* b, const rp_step_params* p, int32_t steps
     if (steps == 0) return RP_OK;
     // the batched kernel runs up to tune.stepsPerLaunch steps per launch;
     // the result is the same as one launch per step
-    const int perLaunch = b->strategy == RP_STRATEGY_BATCHED ? std::max(1, b->tune.stepsPerLaunch) : 1;
+    const int perLaunch =
+        b->strategy == RP_STRATEGY_BATCHED && !b->tune.plain ? std::max(1, b->tune.stepsPerLaunch) : 1;
     auto launchAll = [&]() -> rp_status {
         for (int done = 0; done < steps;) {
             const int k = std::min(perLaunch, steps - done);
@@ -788,7 +704,7 @@ rp_status rp_batch_step_many(rp_batch* b, const rp_step_params* p, int32_t steps
     };
     if (!b->useGraph) return launchAll();
     const bool same = b->graphExec && b->graphSteps == steps && b->graphPrecision == b->precision &&
-                      b->graphStepsPerLaunch == perLaunch &&
+                      b->graphStepsPerLaunch == perLaunch && b->graphPlain == b->tune.plain &&
                       std::memcmp(&b->graphParams, p, sizeof(rp_step_params)) == 0;
     if (!same) {
         if (b->graphExec) {
@@ -814,6 +730,7 @@ rp_status rp_batch_step_many(rp_batch* b, const rp_step_params* p, int32_t steps
         b->graphStepsPerLaunch = perLaunch;
         b->graphParams = *p;
         b->graphPrecision = b->precision;
+        b->graphPlain = b->tune.plain;
     }
     RP_CUDA(cudaGraphLaunch(b->graphExec, b->stream));
     b->launches += b->graphLaunches;
@@ -871,9 +788,9 @@ rp_status rp_batch_set_precision(rp_batch* b, int32_t flags) {
 rp_status rp_batch_get_tuning(const rp_batch* b, int32_t* cta_threads, int32_t* pairs_per_thread,
                               int32_t* steps_per_launch) {
     if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
-    if (cta_threads) *cta_threads = b->tune.ctaThreads;
-    if (pairs_per_thread) *pairs_per_thread = b->tune.pairsPerThread;
-    if (steps_per_launch) *steps_per_launch = b->tune.stepsPerLaunch;
+    if (cta_threads) *cta_threads = b->tune.plain ? 0 : b->tune.ctaThreads;
+    if (pairs_per_thread) *pairs_per_thread = b->tune.plain ? 1 : b->tune.pairsPerThread;
+    if (steps_per_launch) *steps_per_launch = b->tune.plain ? 1 : b->tune.stepsPerLaunch;
     return RP_OK;
 }
 
@@ -881,8 +798,19 @@ rp_status rp_batch_set_tuning(rp_batch* b, int32_t cta_threads, int32_t pairs_pe
                               int32_t steps_per_launch) {
     if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
     if (b->strategy != RP_STRATEGY_BATCHED) return fail(RP_ERR_INVALID, "tuning applies to RP_STRATEGY_BATCHED");
+    if (cta_threads == 0) {  // the plain one-rod-per-CTA kernel
+        rp_status st = syncBatch(b);
+        if (st != RP_OK) return st;
+        if ((st = reservePlain(b)) != RP_OK) return st;
+        b->tune.plain = true;
+        if (b->graphExec) {
+            cudaGraphExecDestroy(b->graphExec);
+            b->graphExec = nullptr;
+        }
+        return RP_OK;
+    }
     if (cta_threads != 128 && cta_threads != 256)
-        return fail(RP_ERR_INVALID, "cta_threads must be 128 or 256");
+        return fail(RP_ERR_INVALID, "cta_threads must be 0 (one rod per CTA), 128 or 256");
     if (pairs_per_thread < 1 || pairs_per_thread > 8)
         return fail(RP_ERR_INVALID, "pairs_per_thread must be in 1..8");
     if (steps_per_launch < 1 || steps_per_launch > 64)
@@ -893,6 +821,7 @@ rp_status rp_batch_set_tuning(rp_batch* b, int32_t cta_threads, int32_t pairs_pe
     want.ctaThreads = cta_threads;
     want.pairsPerThread = pairs_per_thread;
     want.stepsPerLaunch = steps_per_launch;
+    want.plain = false;
     if (want.ctaThreads != b->tune.ctaThreads || want.pairsPerThread != b->tune.pairsPerThread) {
         if ((st = buildBatchedPlan(b, want, b->precision)) != RP_OK) return st;  // batch unchanged
     }
@@ -904,621 +833,9 @@ rp_status rp_batch_set_tuning(rp_batch* b, int32_t cta_threads, int32_t pairs_pe
     return RP_OK;
 }
 
-namespace {
-
-// Device copies of everything a step changes, so tuning trials leave the
-// batch as they found it.
-struct StateSnapshot {
-    std::vector<std::pair<void*, size_t>> regions;
-    std::vector<void*> copies;
-    ~StateSnapshot() {
-        for (void* c : copies) cudaFree(c);
-    }
-    rp_status take(rp_batch* b) {
-        const DArgs& A = b->a;
-        const size_t P = size_t(b->totalP), S = size_t(b->totalS), R = size_t(b->numRods);
-        auto add = [&](const void* p, size_t bytes) {
-            if (p && bytes) regions.emplace_back(const_cast<void*>(p), bytes);
-        };
-        add(A.x, P * 16);
-        add(A.v, P * 16);
-        add(A.xComp, P * 16);
-        add(A.qComp, S * 16);
-        add(A.kinVel, P * 16);
-        add(A.q, S * 16);
-        add(A.omega, S * 16);
-        add(A.contactState, size_t(b->totalSlots));
-        add(A.selfCount, R * 4);
-        add(A.selfOverflow, R * 4);
-        add(A.selfPairs, size_t(b->totalPool) * 4);
-        add(A.errors, R * 4);
-        add(A.rodTime, R * 8);
-        add(A.hold, R * sizeof(rp::DHold));
-        add(A.waypoints, R * sizeof(rp::DWaypoints));  // their step counters advance
-        for (auto& rg : regions) {
-            void* c = nullptr;
-            if (cudaMalloc(&c, rg.second) != cudaSuccess) {
-                cudaGetLastError();
-                return fail(RP_ERR_OUT_OF_MEMORY, "autotune: no room for the state snapshot");
-            }
-            copies.push_back(c);
-            RP_CUDA(cudaMemcpyAsync(c, rg.first, rg.second, cudaMemcpyDeviceToDevice, b->stream));
-        }
-        return RP_OK;
-    }
-    rp_status restore(rp_batch* b) {
-        for (size_t i = 0; i < regions.size(); ++i)
-            RP_CUDA(cudaMemcpyAsync(regions[i].first, copies[i], regions[i].second, cudaMemcpyDeviceToDevice,
-                                    b->stream));
-        return RP_OK;
-    }
-};
-
-// Device milliseconds per step of `launches` launches of `k` steps each.
-rp_status timeSteps(rp_batch* b, const rp_step_params* p, int k, int launches, float* msPerStep) {
-    cudaEvent_t e0, e1;
-    RP_CUDA(cudaEventCreate(&e0));
-    RP_CUDA(cudaEventCreate(&e1));
-    rp_status st = RP_OK;
-    cudaEventRecord(e0, b->stream);
-    for (int i = 0; i < launches && st == RP_OK; ++i) st = launchStep(b, p, k);
-    cudaEventRecord(e1, b->stream);
-    const cudaError_t e = cudaEventSynchronize(e1);
-    float ms = 0.0f;
-    if (st == RP_OK && e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    if (st != RP_OK) return st;
-    if (e != cudaSuccess) return fail(RP_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(e));
-    *msPerStep = ms / float(k * launches);
-    return RP_OK;
-}
-
-}  // namespace
-
-rp_status rp_batch_autotune(rp_batch* b, const rp_step_params* p, int32_t max_steps_per_launch) {
-    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
-    rp_status st = validateParams(p);
-    if (st != RP_OK) return st;
-    if (b->strategy != RP_STRATEGY_BATCHED) return fail(RP_ERR_INVALID, "tuning applies to RP_STRATEGY_BATCHED");
-    if (max_steps_per_launch < 1) return fail(RP_ERR_INVALID, "max_steps_per_launch must be >= 1");
-    if ((st = syncBatch(b)) != RP_OK) return st;
-    StateSnapshot snap;
-    if ((st = snap.take(b)) != RP_OK) return st;
-    const long long launches0 = b->launches;
-    const Tune start = b->tune;
-    Tune best = start;
-    float bestMs = 3.0e38f;
-    // rods per CTA and threads per rod: every (CTA size, team size) pair that
-    // plans, one warm launch and two timed launches from the same state
-    for (int cta : {128, 256}) {
-        for (int ppt : {1, 2}) {
-            Tune trialShape = start;
-            trialShape.ctaThreads = cta;
-            trialShape.pairsPerThread = ppt;
-            trialShape.stepsPerLaunch = 1;
-            if (buildBatchedPlan(b, trialShape, b->precision) != RP_OK) continue;
-            b->tune.stepsPerLaunch = 1;
-            float ms = 0.0f;
-            if ((st = snap.restore(b)) != RP_OK) break;
-            if ((st = launchStep(b, p, 1)) != RP_OK) break;
-            if ((st = snap.restore(b)) != RP_OK) break;
-            if ((st = timeSteps(b, p, 1, 2, &ms)) != RP_OK) break;
-            if (ms < bestMs) {
-                bestMs = ms;
-                best = b->tune;
-            }
-        }
-        if (st != RP_OK) break;
-    }
-    // whole steps per launch, on the chosen shape; a longer launch must win
-    // by 2 % to be kept
-    if (st == RP_OK && bestMs < 3.0e38f) {
-        st = buildBatchedPlan(b, best, b->precision);
-        for (int k = 2; st == RP_OK && k <= max_steps_per_launch && k <= 8; k *= 2) {
-            float ms = 0.0f;
-            if ((st = snap.restore(b)) != RP_OK) break;
-            if ((st = timeSteps(b, p, k, 1, &ms)) != RP_OK) break;
-            if (ms < bestMs * 0.98f) {
-                bestMs = ms;
-                best.stepsPerLaunch = k;
-            }
-        }
-    }
-    const rp_status trial = st;
-    const Tune keep = trial == RP_OK ? best : start;
-    st = buildBatchedPlan(b, keep, b->precision);
-    if (st == RP_OK) b->tune = keep;
-    const rp_status back = snap.restore(b);
-    const rp_status sync = syncBatch(b);
-    b->launches = launches0;
-    if (b->graphExec) {
-        cudaGraphExecDestroy(b->graphExec);
-        b->graphExec = nullptr;
-    }
-    if (trial != RP_OK) return trial;
-    if (st != RP_OK) return st;
-    if (back != RP_OK) return back;
-    if (sync != RP_OK) return sync;
-    if (bestMs >= 3.0e38f) return fail(RP_ERR_SHARED_MEMORY, "autotune: no launch shape fits");
-    return RP_OK;
-}
-
 rp_status rp_batch_set_graph(rp_batch* b, int32_t enabled) {
     if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
     b->useGraph = enabled != 0;
-    return RP_OK;
-}
-
-rp_status rp_batch_download(rp_batch* b, int32_t rod, rp_rod_desc* out) {
-    if (!b || !out) return fail(RP_ERR_INVALID, "batch or out is NULL");
-    if (rod < 0 || rod >= b->numRods) return fail(RP_ERR_INVALID, "rod index out of range");
-    if (!sameTopology(b, rod, out) || !out->x || !out->q)
-        return fail(RP_ERR_INVALID, "out does not have the rod's topology");
-    const DRod& R = b->rods[rod];
-    const int nP = b->tmplNP[rod], nS = b->tmplNS[rod];
-    std::vector<float4> x(nP), v(nP), c(nP), q(nS), w(nS);
-    RP_CUDA(cudaMemcpyAsync(x.data(), b->a.x + R.pOff, nP * sizeof(float4), cudaMemcpyDeviceToHost, b->stream));
-    RP_CUDA(cudaMemcpyAsync(v.data(), b->a.v + R.pOff, nP * sizeof(float4), cudaMemcpyDeviceToHost, b->stream));
-    RP_CUDA(cudaMemcpyAsync(c.data(), b->a.xComp + R.pOff, nP * sizeof(float4), cudaMemcpyDeviceToHost, b->stream));
-    RP_CUDA(cudaMemcpyAsync(q.data(), b->a.q + R.sOff, nS * sizeof(float4), cudaMemcpyDeviceToHost, b->stream));
-    RP_CUDA(cudaMemcpyAsync(w.data(), b->a.omega + R.sOff, nS * sizeof(float4), cudaMemcpyDeviceToHost, b->stream));
-    std::vector<float4> qc(nS, make_float4(0, 0, 0, 0));
-    RP_CUDA(cudaMemcpyAsync(qc.data(), b->a.qComp + R.sOff, nS * sizeof(float4), cudaMemcpyDeviceToHost, b->stream));
-    rp_status st = syncBatch(b);
-    if (st != RP_OK) return st;
-    const bool comp = (b->precision & RP_PRECISION_COMPENSATED) != 0;
-    for (int i = 0; i < nP; ++i) {
-        out->x[3 * i] = double(x[i].x) - (comp ? double(c[i].x) : 0.0);
-        out->x[3 * i + 1] = double(x[i].y) - (comp ? double(c[i].y) : 0.0);
-        out->x[3 * i + 2] = double(x[i].z) - (comp ? double(c[i].z) : 0.0);
-        if (out->v) {
-            out->v[3 * i] = v[i].x;
-            out->v[3 * i + 1] = v[i].y;
-            out->v[3 * i + 2] = v[i].z;
-        }
-    }
-    for (int j = 0; j < nS; ++j) {
-        out->q[4 * j] = double(q[j].x) - (comp ? double(qc[j].x) : 0.0);
-        out->q[4 * j + 1] = double(q[j].y) - (comp ? double(qc[j].y) : 0.0);
-        out->q[4 * j + 2] = double(q[j].z) - (comp ? double(qc[j].z) : 0.0);
-        out->q[4 * j + 3] = double(q[j].w) - (comp ? double(qc[j].w) : 0.0);
-        if (out->omega) {
-            out->omega[3 * j] = w[j].x;
-            out->omega[3 * j + 1] = w[j].y;
-            out->omega[3 * j + 2] = w[j].z;
-        }
-    }
-    return RP_OK;
-}
-
-rp_status rp_batch_download_positions(rp_batch* b, float* out, int64_t cap) {
-    if (!b || !out) return fail(RP_ERR_INVALID, "batch or out is NULL");
-    const size_t P = size_t(b->totalP);
-    if (cap < int64_t(3 * P)) return fail(RP_ERR_INVALID, "capacity below 3 x total particles");
-    std::vector<float4> x(P), c;
-    RP_CUDA(cudaMemcpyAsync(x.data(), b->a.x, P * sizeof(float4), cudaMemcpyDeviceToHost, b->stream));
-    const bool comp = (b->precision & RP_PRECISION_COMPENSATED) != 0;
-    if (comp) {
-        c.resize(P);
-        RP_CUDA(cudaMemcpyAsync(c.data(), b->a.xComp, P * sizeof(float4), cudaMemcpyDeviceToHost, b->stream));
-    }
-    rp_status st = syncBatch(b);
-    if (st != RP_OK) return st;
-    for (size_t i = 0; i < P; ++i) {
-        out[3 * i] = comp ? float(double(x[i].x) - double(c[i].x)) : x[i].x;
-        out[3 * i + 1] = comp ? float(double(x[i].y) - double(c[i].y)) : x[i].y;
-        out[3 * i + 2] = comp ? float(double(x[i].z) - double(c[i].z)) : x[i].z;
-    }
-    return RP_OK;
-}
-
-rp_status rp_batch_download_frames(rp_batch* b, float* out, int64_t cap) {
-    if (!b || !out) return fail(RP_ERR_INVALID, "batch or out is NULL");
-    const size_t S = size_t(b->totalS);
-    if (cap < int64_t(4 * S)) return fail(RP_ERR_INVALID, "capacity below 4 x total frames");
-    std::vector<float4> q(S), c;
-    RP_CUDA(cudaMemcpyAsync(q.data(), b->a.q, S * sizeof(float4), cudaMemcpyDeviceToHost, b->stream));
-    const bool comp = (b->precision & RP_PRECISION_COMPENSATED) != 0;
-    if (comp) {
-        c.resize(S);
-        RP_CUDA(cudaMemcpyAsync(c.data(), b->a.qComp, S * sizeof(float4), cudaMemcpyDeviceToHost, b->stream));
-    }
-    rp_status st = syncBatch(b);
-    if (st != RP_OK) return st;
-    if (comp)
-        for (size_t j = 0; j < S; ++j)
-            q[j] = make_float4(float(double(q[j].x) - c[j].x), float(double(q[j].y) - c[j].y),
-                               float(double(q[j].z) - c[j].z), float(double(q[j].w) - c[j].w));
-    std::memcpy(out, q.data(), S * sizeof(float4));
-    return RP_OK;
-}
-
-static rp_status setLoadsImpl(rp_batch* b, int rod, const rp_rod_desc* s) {
-    const DRod& R = b->rods[rod];
-    const int nP = b->tmplNP[rod], nS = b->tmplNS[rod];
-    std::vector<float4> f(nP), k(nP), t(nS), q(nS);
-    packParticles(s, nullptr, nullptr, f.data(), k.data());
-    packFrames(s, q.data(), nullptr, t.data());
-    RP_CUDA(cudaMemcpyAsync(b->a.force + R.pOff, f.data(), nP * sizeof(float4), cudaMemcpyHostToDevice, b->stream));
-    RP_CUDA(cudaMemcpyAsync(b->a.kinVel + R.pOff, k.data(), nP * sizeof(float4), cudaMemcpyHostToDevice, b->stream));
-    RP_CUDA(cudaMemcpyAsync(b->a.torque + R.sOff, t.data(), nS * sizeof(float4), cudaMemcpyHostToDevice, b->stream));
-    // fixed frames (zero inertia) take their orientation from the source:
-    // how an end is driven, e.g. twisted (gpu_batch.cpp:386-389)
-    const std::vector<char>& fixed = b->fixedFrame[R.tmpl];
-    // compensated precision: the driven frame's rounding error goes to qComp,
-    // so the imposed orientation is carried to FP64 accuracy
-    const bool comp = (b->precision & RP_PRECISION_COMPENSATED) != 0;
-    std::vector<float4> qc(nS, make_float4(0, 0, 0, 0));
-    for (int j = 0; j < nS && comp; ++j) {
-        const double* src = s->q + 4 * j;  // w, x, y, z
-        qc[j] = make_float4(float(double(q[j].x) - src[0]), float(double(q[j].y) - src[1]),
-                            float(double(q[j].z) - src[2]), float(double(q[j].w) - src[3]));
-    }
-    for (int j = 0; j < nS; ++j)
-        if (fixed[j]) {
-            RP_CUDA(cudaMemcpyAsync(b->a.q + R.sOff + j, &q[j], sizeof(float4), cudaMemcpyHostToDevice, b->stream));
-            RP_CUDA(cudaMemcpyAsync(b->a.qComp + R.sOff + j, &qc[j], sizeof(float4), cudaMemcpyHostToDevice,
-                                    b->stream));
-        }
-    return syncBatch(b);
-}
-
-rp_status rp_batch_set_loads(rp_batch* b, int32_t rod, const rp_rod_desc* s) {
-    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
-    if (rod < 0 || rod >= b->numRods) return fail(RP_ERR_INVALID, "rod index out of range");
-    if (!sameTopology(b, rod, s) || !s->q) return fail(RP_ERR_INVALID, "source does not have the rod's topology");
-    return setLoadsImpl(b, rod, s);
-}
-
-// Compensation of freshly uploaded state: zero in reference order; with
-// compensated precision the rounding residual of each double input (float
-// value minus the double), so that value - compensation is the input exactly.
-static void uploadResiduals(const rp_batch* b, const rp_rod_desc* s, const float4* x, const float4* q,
-                            float4* xc, float4* qc) {
-    const bool comp = (b->precision & RP_PRECISION_COMPENSATED) != 0;
-    for (int i = 0; i < s->num_particles; ++i) {
-        const double* p = s->x + 3 * i;
-        xc[i] = comp ? make_float4(float(double(x[i].x) - p[0]), float(double(x[i].y) - p[1]),
-                                   float(double(x[i].z) - p[2]), 0.0f)
-                     : make_float4(0, 0, 0, 0);
-    }
-    for (int j = 0; j < s->num_frames; ++j) {
-        const double* p = s->q + 4 * j;  // w, x, y, z as q[j].x .. q[j].w
-        qc[j] = comp ? make_float4(float(double(q[j].x) - p[0]), float(double(q[j].y) - p[1]),
-                                   float(double(q[j].z) - p[2]), float(double(q[j].w) - p[3]))
-                     : make_float4(0, 0, 0, 0);
-    }
-}
-
-static rp_status uploadRodImpl(rp_batch* b, int rod, const rp_rod_desc* s) {
-    const DRod& R = b->rods[rod];
-    const int nP = b->tmplNP[rod], nS = b->tmplNS[rod];
-    std::vector<float4> x(nP), v(nP), q(nS), w(nS), xc(nP), qc(nS);
-    packParticles(s, x.data(), v.data(), nullptr, nullptr);
-    packFrames(s, q.data(), w.data(), nullptr);
-    uploadResiduals(b, s, x.data(), q.data(), xc.data(), qc.data());
-    RP_CUDA(cudaMemcpyAsync(b->a.x + R.pOff, x.data(), nP * sizeof(float4), cudaMemcpyHostToDevice, b->stream));
-    RP_CUDA(cudaMemcpyAsync(b->a.v + R.pOff, v.data(), nP * sizeof(float4), cudaMemcpyHostToDevice, b->stream));
-    RP_CUDA(cudaMemcpyAsync(b->a.xComp + R.pOff, xc.data(), nP * sizeof(float4), cudaMemcpyHostToDevice, b->stream));
-    RP_CUDA(cudaMemcpyAsync(b->a.q + R.sOff, q.data(), nS * sizeof(float4), cudaMemcpyHostToDevice, b->stream));
-    RP_CUDA(cudaMemcpyAsync(b->a.qComp + R.sOff, qc.data(), nS * sizeof(float4), cudaMemcpyHostToDevice, b->stream));
-    RP_CUDA(cudaMemcpyAsync(b->a.omega + R.sOff, w.data(), nS * sizeof(float4), cudaMemcpyHostToDevice, b->stream));
-    return setLoadsImpl(b, rod, s);
-}
-
-rp_status rp_batch_upload_rod(rp_batch* b, int32_t rod, const rp_rod_desc* s) {
-    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
-    if (rod < 0 || rod >= b->numRods) return fail(RP_ERR_INVALID, "rod index out of range");
-    if (!sameTopology(b, rod, s) || !s->x || !s->q)
-        return fail(RP_ERR_INVALID, "source does not have the rod's topology");
-    return uploadRodImpl(b, rod, s);
-}
-
-rp_status rp_batch_upload(rp_batch* b, const rp_rod_desc* s) {
-    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
-    for (int r = 0; r < b->numRods; ++r) {
-        if (!sameTopology(b, r, s) || !s->x || !s->q)
-            return fail(RP_ERR_INVALID, "source does not have rod " + std::to_string(r) + "'s topology");
-    }
-    const size_t P = size_t(b->totalP), S = size_t(b->totalS);
-    std::vector<float4> hx(P), hv(P), hf(P), hk(P), hq(S), hw(S), ht(S), hxc(P), hqc(S);
-    for (int r = 0; r < b->numRods; ++r) {
-        const DRod& R = b->rods[r];
-        packParticles(s, &hx[R.pOff], &hv[R.pOff], &hf[R.pOff], &hk[R.pOff]);
-        packFrames(s, &hq[R.sOff], &hw[R.sOff], &ht[R.sOff]);
-        uploadResiduals(b, s, &hx[R.pOff], &hq[R.sOff], &hxc[R.pOff], &hqc[R.sOff]);
-    }
-    rp_status st;
-    if ((st = b->upload(b->a.x, hx)) || (st = b->upload(b->a.v, hv)) || (st = b->upload(b->a.force, hf)) ||
-        (st = b->upload(b->a.kinVel, hk)) || (st = b->upload(b->a.q, hq)) || (st = b->upload(b->a.omega, hw)) ||
-        (st = b->upload(b->a.torque, ht)) || (st = b->upload(b->a.xComp, hxc)) || (st = b->upload(b->a.qComp, hqc)))
-        return st;
-    return syncBatch(b);
-}
-
-rp_status rp_batch_set_kinematic_velocities(rp_batch* b, const float* xyz, int64_t count) {
-    if (!b || !xyz) return fail(RP_ERR_INVALID, "batch or data is NULL");
-    if (count != b->totalP) return fail(RP_ERR_INVALID, "count must equal the total particle count");
-    std::vector<float4> k(static_cast<size_t>(count));
-    for (int64_t i = 0; i < count; ++i) k[i] = make_float4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], 0.0f);
-    rp_status st = b->upload(b->a.kinVel, k);
-    if (st != RP_OK) return st;
-    return syncBatch(b);
-}
-
-rp_status rp_batch_set_material_scales(rp_batch* b, const float* youngs, const float* friction, int32_t n) {
-    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
-    if ((youngs || friction) && n != b->numRods) return fail(RP_ERR_INVALID, "n must equal num_rods");
-    if (youngs) {
-        std::vector<float> c(n);
-        for (int r = 0; r < n; ++r) {
-            if (!(youngs[r] > 0)) return fail(RP_ERR_INVALID, "youngs_scale must be positive");
-            c[r] = 1.0f / youngs[r];
-        }
-        rp_status st = b->upload(const_cast<float*>(b->a.complianceScale), c);
-        if (st != RP_OK) return st;
-    }
-    if (friction) {
-        std::vector<float> f(friction, friction + n);
-        rp_status st = b->upload(const_cast<float*>(b->a.frictionScale), f);
-        if (st != RP_OK) return st;
-    }
-    return syncBatch(b);
-}
-
-rp_status rp_batch_set_drives(rp_batch* b, const rp_drive* drives, int32_t n) {
-    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
-    if (!drives) {
-        b->a.drives = nullptr;
-        return RP_OK;
-    }
-    if (n != b->numRods) return fail(RP_ERR_INVALID, "n must equal num_rods");
-    std::vector<rp::DDrive> d(n);
-    for (int r = 0; r < n; ++r) {
-        d[r].particle = drives[r].particle;
-        if (d[r].particle >= b->tmplNP[r]) return fail(RP_ERR_INVALID, "drive particle out of range");
-        d[r].ax = drives[r].axis[0];
-        d[r].ay = drives[r].axis[1];
-        d[r].az = drives[r].axis[2];
-        d[r].amplitude = drives[r].amplitude;
-        d[r].omega = float(2.0 * 3.14159265358979323846 * double(drives[r].frequency));
-        d[r].phase = drives[r].phase;
-    }
-    rp::DDrive* dd = b->driveStore;
-    if (!dd) {
-        rp_status st = b->alloc(dd, size_t(n));
-        if (st != RP_OK) return st;
-        b->driveStore = dd;
-    }
-    rp_status st = b->upload(dd, d);
-    if (st != RP_OK) return st;
-    b->a.drives = dd;
-    b->a.waypoints = nullptr;  // one kind of drive at a time
-    if (b->graphExec) {
-        cudaGraphExecDestroy(b->graphExec);
-        b->graphExec = nullptr;
-    }
-    return syncBatch(b);
-}
-
-rp_status rp_batch_set_waypoint_drives(rp_batch* b, const rp_waypoint_drive* drives, int32_t n) {
-    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
-    auto dropGraph = [&]() {
-        if (b->graphExec) {
-            cudaGraphExecDestroy(b->graphExec);
-            b->graphExec = nullptr;
-        }
-    };
-    if (!drives) {
-        if (b->a.waypoints) dropGraph();
-        b->a.waypoints = nullptr;
-        return RP_OK;
-    }
-    if (n != b->numRods) return fail(RP_ERR_INVALID, "n must equal num_rods");
-    static_assert(rp::kMaxWaypoints == RP_MAX_WAYPOINTS, "waypoint capacity");
-    std::vector<rp::DWaypoints> w(n);
-    for (int r = 0; r < n; ++r) {
-        const rp_waypoint_drive& d = drives[r];
-        rp::DWaypoints& o = w[r];
-        o.particle = d.particle;
-        o.count = d.count;
-        o.stepsPerControl = d.steps_per_control;
-        o.step = 0;
-        o.dt = d.dt;
-        o.sx = d.start[0];
-        o.sy = d.start[1];
-        o.z = d.height;
-        if (d.particle >= b->tmplNP[r]) return fail(RP_ERR_INVALID, "waypoint drive particle out of range");
-        if (d.particle < 0) continue;
-        if (d.count < 1 || d.count > RP_MAX_WAYPOINTS)
-            return fail(RP_ERR_INVALID, "waypoint count must be 1.." + std::to_string(RP_MAX_WAYPOINTS));
-        if (d.steps_per_control < 1) return fail(RP_ERR_INVALID, "steps_per_control must be >= 1");
-        if (!(d.dt > 0) || !std::isfinite(d.dt)) return fail(RP_ERR_INVALID, "waypoint dt must be > 0");
-        for (int k = 0; k < RP_MAX_WAYPOINTS; ++k) {
-            const bool used = k < d.count;
-            if (used && (!(d.legs[k] > 0) || !std::isfinite(d.legs[k])))
-                return fail(RP_ERR_INVALID, "waypoint legs must be > 0");
-            o.legs[k] = used ? d.legs[k] : 0.0;
-            o.wx[k] = used ? d.waypoints[k][0] : 0.0;
-            o.wy[k] = used ? d.waypoints[k][1] : 0.0;
-        }
-    }
-    rp::DWaypoints* dw = b->waypointStore;
-    if (!dw) {
-        rp_status st = b->alloc(dw, size_t(n));
-        if (st != RP_OK) return st;
-        b->waypointStore = dw;
-    }
-    rp_status st = b->upload(dw, w);
-    if (st != RP_OK) return st;
-    // a captured graph holds the step arguments: it stays valid while they
-    // point at the same arrays, whose contents the kernels read at run time
-    if (b->a.waypoints != dw || b->a.drives) dropGraph();
-    b->a.waypoints = dw;
-    b->a.drives = nullptr;  // one kind of drive at a time
-    return syncBatch(b);
-}
-
-rp_status rp_batch_evaluate_harness(rp_batch* b, const rp_harness_board* board, rp_harness_outcome* out,
-                                    int32_t n) {
-    if (!b || !board || !out) return fail(RP_ERR_INVALID, "batch, board or out is NULL");
-    if (n != b->numRods) return fail(RP_ERR_INVALID, "n must equal num_rods");
-    static_assert(sizeof(rp_harness_outcome) == sizeof(rp::DOutcome), "outcome layout");
-    rp::DBoard B;
-    B.ax = board->peg_a[0];
-    B.ay = board->peg_a[1];
-    B.bx = board->peg_b[0];
-    B.by = board->peg_b[1];
-    B.cx = board->clip[0];
-    B.cy = board->clip[1];
-    B.pegRadius = board->peg_radius;
-    B.clipHalfGap = board->clip_half_gap;
-    B.clipHeight = board->clip_height;
-    B.radius = board->cable_radius;
-    B.slack = board->lay_slack;
-    if (!b->outcomes) {
-        rp_status st = b->alloc(b->outcomes, size_t(b->numRods), false);
-        if (st != RP_OK) return st;
-    }
-    const int comp = (b->precision & RP_PRECISION_COMPENSATED) != 0;
-    RP_CUDA(rp::launchEvaluateHarness(b->a, B, comp, b->outcomes, b->stream));
-    RP_CUDA(cudaMemcpyAsync(out, b->outcomes, size_t(n) * sizeof(rp::DOutcome), cudaMemcpyDeviceToHost,
-                            b->stream));
-    return syncBatch(b);
-}
-
-rp_status rp_batch_set_time(rp_batch* b, double t) {
-    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
-    std::vector<double> tt(b->numRods, t);
-    rp_status st = b->upload(b->a.rodTime, tt);
-    if (st != RP_OK) return st;
-    return syncBatch(b);
-}
-
-rp_status rp_batch_read_state_async(rp_batch* b, int32_t what, void* dst, int64_t bytes) {
-    if (!b || !dst) return fail(RP_ERR_INVALID, "batch or dst is NULL");
-    const void* src = nullptr;
-    int64_t size = 0;
-    switch (what) {
-        case RP_STATE_POSITIONS: src = b->a.x; size = b->totalP * 16; break;
-        case RP_STATE_FRAMES: src = b->a.q; size = b->totalS * 16; break;
-        case RP_STATE_CONTACTS: src = b->a.contactState; size = b->totalSlots; break;
-        default: return fail(RP_ERR_INVALID, "unknown state array for reading");
-    }
-    if (bytes != size) return fail(RP_ERR_INVALID, "bytes must be " + std::to_string(size));
-    if (size > 0) RP_CUDA(cudaMemcpyAsync(dst, src, size_t(size), cudaMemcpyDeviceToHost, b->stream));
-    return RP_OK;
-}
-
-rp_status rp_batch_write_state_async(rp_batch* b, int32_t what, const void* src, int64_t bytes) {
-    if (!b || !src) return fail(RP_ERR_INVALID, "batch or src is NULL");
-    if (what != RP_STATE_KINEMATIC) return fail(RP_ERR_INVALID, "only RP_STATE_KINEMATIC is writable");
-    const int64_t size = b->totalP * 16;
-    if (bytes != size) return fail(RP_ERR_INVALID, "bytes must be " + std::to_string(size));
-    RP_CUDA(cudaMemcpyAsync(b->a.kinVel, src, size_t(size), cudaMemcpyHostToDevice, b->stream));
-    return RP_OK;
-}
-
-rp_status rp_batch_read_contact_states(rp_batch* b, uint8_t* out, int64_t cap, int64_t* count) {
-    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
-    if (count) *count = b->totalSlots;
-    if (!out) return RP_OK;
-    if (cap < b->totalSlots) return fail(RP_ERR_INVALID, "capacity below the slot count");
-    if (b->totalSlots > 0)
-        RP_CUDA(cudaMemcpyAsync(out, b->a.contactState, size_t(b->totalSlots), cudaMemcpyDeviceToHost, b->stream));
-    return syncBatch(b);
-}
-
-rp_status rp_batch_read_self_contacts(rp_batch* b, int32_t rod, int32_t* pairs, int32_t cap, int32_t* count) {
-    if (!b || !count) return fail(RP_ERR_INVALID, "batch or count is NULL");
-    if (rod < 0 || rod >= b->numRods) return fail(RP_ERR_INVALID, "rod index out of range");
-    const DRod& R = b->rods[rod];
-    *count = 0;
-    if (!R.selfCollision) return RP_OK;
-    int32_t live = 0;
-    RP_CUDA(cudaMemcpyAsync(&live, b->a.selfCount + rod, sizeof(int32_t), cudaMemcpyDeviceToHost, b->stream));
-    rp_status st = syncBatch(b);
-    if (st != RP_OK) return st;
-    *count = live;
-    if (!pairs || live == 0) return RP_OK;
-    if (cap < live) return fail(RP_ERR_INVALID, "capacity below the pair count");
-    std::vector<int32_t> enc(live);
-    RP_CUDA(cudaMemcpyAsync(enc.data(), b->a.selfPairs + R.poolOff, live * sizeof(int32_t),
-                            cudaMemcpyDeviceToHost, b->stream));
-    if ((st = syncBatch(b)) != RP_OK) return st;
-    for (int c = 0; c < live; ++c) {
-        pairs[2 * c] = enc[c] >> 16;
-        pairs[2 * c + 1] = enc[c] & 0xffff;
-    }
-    return RP_OK;
-}
-
-rp_status rp_batch_arm_hold_observer(rp_batch* b, const int32_t* particle, int32_t n, int32_t interval,
-                                     double tolerance) {
-    if (!b || !particle) return fail(RP_ERR_INVALID, "batch or particle is NULL");
-    if (n != b->numRods || interval < 1) return fail(RP_ERR_INVALID, "n must equal num_rods, interval >= 1");
-    const size_t P = size_t(b->totalP);
-    std::vector<float4> x(P), c(P);
-    RP_CUDA(cudaMemcpyAsync(x.data(), b->a.x, P * sizeof(float4), cudaMemcpyDeviceToHost, b->stream));
-    RP_CUDA(cudaMemcpyAsync(c.data(), b->a.xComp, P * sizeof(float4), cudaMemcpyDeviceToHost, b->stream));
-    rp_status st = syncBatch(b);
-    if (st != RP_OK) return st;
-    const bool comp = (b->precision & RP_PRECISION_COMPENSATED) != 0;
-    std::vector<rp::DHold> h(n);
-    for (int r = 0; r < n; ++r) {
-        h[r].particle = particle[r];
-        if (particle[r] >= b->tmplNP[r]) return fail(RP_ERR_INVALID, "observer particle out of range");
-        h[r].steps = 0;
-        h[r].maxRise = 0.0;
-        h[r].startZ = 0.0;
-        if (particle[r] >= 0) {
-            const size_t i = size_t(b->rods[r].pOff) + particle[r];
-            h[r].startZ = double(x[i].z) - (comp ? double(c[i].z) : 0.0);
-        }
-    }
-    if (!b->a.hold) {
-        rp::DHold* dh = nullptr;
-        if ((st = b->alloc(dh, size_t(n))) != RP_OK) return st;
-        b->a.hold = dh;
-    }
-    if ((st = b->upload(b->a.hold, h)) != RP_OK) return st;
-    b->a.holdInterval = interval;
-    b->holdInterval = interval;
-    b->holdTolerance = tolerance;
-    b->holdArmed = true;
-    if (b->graphExec) {
-        cudaGraphExecDestroy(b->graphExec);
-        b->graphExec = nullptr;
-    }
-    return syncBatch(b);
-}
-
-rp_status rp_batch_read_hold_verdicts(rp_batch* b, double* maxRise, uint8_t* held, uint8_t* nearBoundary,
-                                      int32_t n) {
-    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
-    if (!b->holdArmed) return fail(RP_ERR_INVALID, "hold observer not armed");
-    if (n != b->numRods) return fail(RP_ERR_INVALID, "n must equal num_rods");
-    // final sample of the run (the reference samples at the last step too,
-    // application_cases.cpp:59)
-    const cudaError_t e = rp::launchObserve(b->a, (b->precision & RP_PRECISION_COMPENSATED) != 0, b->stream);
-    if (e != cudaSuccess) return fail(RP_ERR_CUDA, cudaGetErrorString(e));
-    b->launches += 1;
-    std::vector<rp::DHold> h(n);
-    RP_CUDA(cudaMemcpyAsync(h.data(), b->a.hold, n * sizeof(rp::DHold), cudaMemcpyDeviceToHost, b->stream));
-    rp_status st = syncBatch(b);
-    if (st != RP_OK) return st;
-    for (int r = 0; r < n; ++r) {
-        if (maxRise) maxRise[r] = h[r].maxRise;
-        if (held) held[r] = h[r].maxRise <= b->holdTolerance ? 1 : 0;
-        if (nearBoundary) {
-            // within a few float spacings of the threshold at the observed height
-            const float zf = float(h[r].startZ + b->holdTolerance);
-            const double spacing = double(std::nextafter(std::fabs(zf), 2.0f * std::fabs(zf) + 1.0f)) -
-                                   double(std::fabs(zf));
-            nearBoundary[r] = std::fabs(h[r].maxRise - b->holdTolerance) <= 4.0 * spacing ? 1 : 0;
-        }
-    }
     return RP_OK;
 }
 

@@ -31,8 +31,10 @@
 // results are bit-identical to the plain kernel.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <mutex>
 
+#include "rp_bulk.cuh"
 #include "rp_launch.h"
 #include "rp_layout.h"
 #include "rp_step_common.cuh"
@@ -178,13 +180,155 @@ __device__ void countSelfByBlocks(const RodView& V, const SelfScratch& S, int nS
     }
 }
 
+// Everything a team needs about its rod beyond the shared arrays: the views
+// of its arrays, its scratch words and colour tables, its drive. Lane 0 writes
+// it once per rod into shared memory and every phase reads the fields it
+// uses, so the substep loop carries only the current phase's values in
+// registers (held in registers, these pointers alone filled a third of the
+// register file and pushed the constraint arithmetic into spills).
+struct TeamCtx {
+    RodView V;
+    SelfScratch S;
+    int32_t* cursor;                // hash placement cursors (table entries)
+    int32_t* partial;               // scan partials, one per warp
+    int32_t* numLevels;             // projection levels of the pool
+    unsigned long long* primMask;   // this substep's primitive cull
+    int32_t* touching;              // some segment pair touches this substep
+    float* red;                     // per-warp reduction rows, 8 floats each
+    int32_t* lvlOrder;
+    int32_t* lvlStart;
+    int32_t* lvlOf;
+    const int* sOrder;
+    const int* bOrder;
+    const int* sCol;
+    const int* bCol;
+    DDrive drive;
+    double tRod;                    // the rod's simulated time (lane 0 advances it)
+    int32_t driveP, wayP, wayStep;  // driven particle, waypoint particle and step
+    int32_t stageFailed;            // a lane gave up waiting for the staged state
+    uint64_t bar;                   // mbarrier of the rod's bulk stage-in
+};
+
+// Polls of the stage-in barrier before a lane gives up (each poll may wait a
+// while in hardware): far beyond any real copy, so it ends only a broken one.
+constexpr int kStageTries = 1 << 20;
+// DArgs::errors bit of a rod whose state copy never completed
+constexpr int32_t kErrorStage = 2;
+
+// One context per team: a 256-thread CTA holds at most eight one-warp teams.
+constexpr int kMaxTeamsPerCta = 8;
+
+// The pool fill of a substep on which some segment pair touches: the
+// reference's hash (a stable counting sort), its fill pass in bucket order,
+// and the projection levels (or colours) of the pool. Not inlined: it runs
+// only on substeps with a touching pair, and inlined its registers would
+// count against every phase of the substep loop.
+__device__ __noinline__ void fillSelfPool(const TeamCtx& C, int nSt, int nP, int table, float cell, int live,
+                                          int selfGap, int selfCapacity, float selfFriction, int precision,
+                                          int32_t* errorWord, int lane, int team, int teamIdx) {
+    const RodView& V = C.V;
+    const SelfScratch& S = C.S;
+    int32_t* const& cursor = C.cursor;
+    int32_t* const& partial = C.partial;
+    int32_t* const& numLevels = C.numLevels;
+    int32_t* const& lvlOrder = C.lvlOrder;
+    int32_t* const& lvlStart = C.lvlStart;
+    int32_t* const& lvlOf = C.lvlOf;
+        // ---- fill, in the reference's order: its hash buckets ----
+        for (int t = lane; t <= table; t += team) S.cellStart[t] = 0;
+        for (int c = lane; c < live; c += team) S.pool[c].seg = -1;
+        teamSync(team, teamIdx);
+        for (int j = lane; j < nSt; j += team) {
+            const float4 c = S.centres[j];
+            const int h0 = int(hashCell(cellCoord(c.x, cell), cellCoord(c.y, cell),
+                                        cellCoord(c.z, cell), table));
+            S.cellOf[j] = h0;
+            atomicAdd(&S.cellStart[h0], 1);
+        }
+        teamSync(team, teamIdx);
+        // counts -> starts: cellStart[t] = first slot of bucket t,
+        // cellStart[table] = segment count (the reference's offsets)
+        teamExclusiveScan(S.cellStart, table + 1, lane, team, teamIdx, partial);
+        for (int t = lane; t < table; t += team) cursor[t] = S.cellStart[t];
+        teamSync(team, teamIdx);
+        // stable placement, one warp walking segments in order
+        if (lane < 32) {
+            for (int j0 = 0; j0 < nSt; j0 += 32) {
+                const int j = j0 + lane;
+                const bool valid = j < nSt;
+                const int c = valid ? S.cellOf[j] : -1 - lane;
+                const unsigned peers = __match_any_sync(0xffffffffu, c);
+                const int rank = __popc(peers & ((1u << lane) - 1u));
+                const int start = valid ? cursor[c] : 0;
+                __syncwarp();
+                if (valid) {
+                    S.sorted[start + rank] = j;
+                    if (rank == 0) cursor[c] = start + __popc(peers);
+                }
+                __syncwarp();
+            }
+        }
+        teamSync(team, teamIdx);
+        for (int j = lane; j < nSt; j += team)
+            if (S.segCount[j] > 0 && S.segStart[j] < selfCapacity)
+                querySelfSegment<true>(V, S, j, nSt, selfGap, table, selfCapacity,
+                                       selfFriction, true);
+        // every thread is done reading the hash (sorted) before
+        // cellOf and sorted (2 nSt >= nP ints) are reused below
+        teamSync(team, teamIdx);
+        for (int i = lane; i < nP; i += team) S.cellOf[i] = 0;
+        teamSync(team, teamIdx);
+        if (lane == 0) {
+            int kept = live;
+            int n = buildProjectionLevels(S.pool, live, nP, S.cellOf, lvlOf, lvlOrder,
+                                          lvlStart, &kept);
+            if (precision & kPrecisionColoredSelf) {
+                // colours instead of levels (the valid prefix is known now)
+                for (int i = 0; i < nP; ++i) S.cellOf[i] = 0;
+                const int nc = buildProjectionColors(S.pool, kept, S.cellOf, lvlOf, lvlOrder,
+                                                     lvlStart);
+                if (nc >= 0) {
+                    n = nc;
+                } else {  // more than 32 colours: keep the levels
+                    for (int i = 0; i < nP; ++i) S.cellOf[i] = 0;
+                    n = buildProjectionLevels(S.pool, kept, nP, S.cellOf, lvlOf, lvlOrder,
+                                              lvlStart, &kept);
+                }
+            }
+            *numLevels = n;
+            if (kept != live) {
+                // an entry indexed outside the rod or left unwritten:
+                // keep the valid prefix and report it, never touch
+                // memory with it
+                *S.live = kept;
+                if (errorWord) atomicOr(errorWord, 1);
+            }
+        }
+}
+
+// The self-contact pool projected level by level: contacts of one level
+// share no particle, and every earlier contact a contact shares a particle
+// with sits in a lower level -- the serial pool order's result, bit for bit.
+// Not inlined, for the same reason as the fill: it runs only while contacts
+// are live.
+template <bool COMP>
+__device__ __noinline__ void projectSelfLevels(const TeamCtx& C, int nl, int lane, int team, int teamIdx) {
+    for (int l = 0; l < nl; ++l) {
+        for (int c = C.lvlStart[l] + lane; c < C.lvlStart[l + 1]; c += team)
+            projectSelf<COMP>(C.V, C.S.pool[C.lvlOrder[c]]);
+        teamSync(team, teamIdx);
+    }
+}
+
 template <bool COMP, bool FP64>
-__device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int team, int teamIdx) {
+__device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int team, int teamIdx,
+                       TeamCtx* ctxs) {
     const DRod R = A.rods[r];
     const DTemplate T = A.tmpl[R.tmpl];
     const int nP = T.nP, nS = T.nS, nSt = T.nSt, nB = T.nB;
 
-    RodView V;
+    RodView Vb;  // built here, read through the shared context below
+#define V Vb
     V.invMass = A.tInvMass + T.pOff;
     V.invInertia = A.tInvInertia + T.sOff;
     V.inertia = A.tInertia + T.sOff;
@@ -220,85 +364,110 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
     V.lamS = reinterpret_cast<float4*>(base + L.lamS);
     V.lamB = reinterpret_cast<float4*>(base + L.lamB);
     V.slots = A.slotsShared ? reinterpret_cast<DSlot*>(base + L.slots) : A.gSlots + R.slotOff;
-    SelfScratch S;
+    SelfScratch Sb;
+#define S Sb
     S.centres = reinterpret_cast<float4*>(base + L.centres);
     S.cellOf = reinterpret_cast<int32_t*>(base + L.selfInt);
     S.sorted = S.cellOf + nSt;
     S.segCount = S.sorted + nSt;
     S.segStart = S.segCount + nSt;
     S.cellStart = reinterpret_cast<int32_t*>(base + L.hash);
-    int32_t* cursor = S.cellStart + (R.hashTableSize + 1);
     S.pool = A.gPool + R.poolOff;
     int32_t* misc = reinterpret_cast<int32_t*>(base + L.misc);
     S.cellSize = reinterpret_cast<float*>(misc);
     S.live = misc + 1;
     S.overflow = misc + 2;
     S.blocks = reinterpret_cast<float4*>(base + L.blocks);
-    int32_t* partial = misc + 4;  // one per warp of the team (up to 8)
-    int32_t* numLevels = misc + 3;
-    unsigned long long* primMask = reinterpret_cast<unsigned long long*>(misc + 12);
-    int32_t* touching = misc + 14;  // some segment pair touches this substep
-    float* red = reinterpret_cast<float*>(misc + 16);  // 8 floats per warp
-    int32_t* lvlOrder = reinterpret_cast<int32_t*>(base + L.levels);
-    int32_t* lvlStart = lvlOrder + (R.selfCapacity + 1);
-    int32_t* lvlOf = lvlStart + (R.selfCapacity + 1);
+#undef V
+#undef S
+    TeamCtx& C = ctxs[teamIdx];
     if (lane == 0) {
-        *numLevels = 0;
-        *primMask = ~0ull;
+        C.V = Vb;
+        C.S = Sb;
+        C.cursor = Sb.cellStart + (R.hashTableSize + 1);
+        C.partial = misc + 4;  // one per warp of the team (up to 8)
+        C.numLevels = misc + 3;
+        C.primMask = reinterpret_cast<unsigned long long*>(misc + 12);
+        C.touching = misc + 14;
+        C.red = reinterpret_cast<float*>(misc + 16);  // 8 floats per warp
+        C.lvlOrder = reinterpret_cast<int32_t*>(base + L.levels);
+        C.lvlStart = C.lvlOrder + (R.selfCapacity + 1);
+        C.lvlOf = C.lvlStart + (R.selfCapacity + 1);
+        C.sOrder = A.tOrder + T.sOrderOff;
+        C.bOrder = A.tOrder + T.bOrderOff;
+        C.sCol = A.tColorStart + T.sColorOff;
+        C.bCol = A.tColorStart + T.bColorOff;
+        *C.numLevels = 0;
+        *C.primMask = ~0ull;
+        // simulated time of this rod, advanced per step exactly as the
+        // one-step-per-launch path advances rodTime[r]
+        C.tRod = A.rodTime[r];
+        C.driveP = -1;
+        C.drive = DDrive{};
+        if (A.drives) {
+            C.drive = A.drives[r];
+            if (C.drive.particle >= 0 && C.drive.particle < nP) C.driveP = C.drive.particle;
+        }
+        C.wayP = -1;  // waypoint schedule: its particle and step count
+        C.wayStep = 0;
+        if (A.waypoints) {
+            const DWaypoints& W = A.waypoints[r];
+            if (W.particle >= 0 && W.particle < nP) {
+                C.wayP = W.particle;
+                C.wayStep = W.step;
+            }
+        }
     }
+    teamSync(team, teamIdx);
+    const RodView& V = C.V;
+    const SelfScratch& S = C.S;
+    int32_t* const& partial = C.partial;
+    int32_t* const& numLevels = C.numLevels;
+    unsigned long long* const& primMask = C.primMask;
+    int32_t* const& touching = C.touching;
+    float* const& red = C.red;
+    const int* const& sOrder = C.sOrder;
+    const int* const& bOrder = C.bOrder;
+    const int* const& sCol = C.sCol;
+    const int* const& bCol = C.bCol;
 
-    // simulated time of this rod, advanced per step exactly as the
-    // one-step-per-launch path advances rodTime[r]
-    double tRod = A.rodTime[r];
-    int driveP = -1;
-    DDrive drive{};
-    if (A.drives) {
-        drive = A.drives[r];
-        if (drive.particle >= 0 && drive.particle < nP) driveP = drive.particle;
-    }
-    int wayP = -1, wayStep = 0;  // waypoint schedule: its particle and step count
-    if (A.waypoints) {
-        const DWaypoints& W = A.waypoints[r];
-        if (W.particle >= 0 && W.particle < nP) {
-            wayP = W.particle;
-            wayStep = W.step;
+    // ---- stage in: one bulk copy per state array, on the team's mbarrier ----
+    const uint32_t pBytes = uint32_t(nP) * 16u, sBytes = uint32_t(nS) * 16u;
+    if (lane == 0) {
+        C.stageFailed = 0;
+        mbarInit(&C.bar);
+        mbarArriveExpectTx(&C.bar, 2u * pBytes + 2u * sBytes + (COMP ? pBytes + sBytes : 0u));
+        bulkLoad(V.x, A.x + R.pOff, pBytes, &C.bar);
+        bulkLoad(V.v, A.v + R.pOff, pBytes, &C.bar);
+        bulkLoad(V.q, A.q + R.sOff, sBytes, &C.bar);
+        bulkLoad(V.omega, A.omega + R.sOff, sBytes, &C.bar);
+        if (COMP) {
+            bulkLoad(V.xComp, A.xComp + R.pOff, pBytes, &C.bar);
+            bulkLoad(V.qComp, A.qComp + R.sOff, sBytes, &C.bar);
         }
     }
-
-    // ---- stage in (coalesced float4 rows) ----
-    {
-        const float4* gx = A.x + R.pOff;
-        const float4* gv = A.v + R.pOff;
-        const float4* gc = A.xComp + R.pOff;
-        for (int i = lane; i < nP; i += team) {
-            V.x[i] = gx[i];
-            V.v[i] = gv[i];
-            if (COMP) V.xComp[i] = gc[i];
-        }
-        const float4* gq = A.q + R.sOff;
-        const float4* gw = A.omega + R.sOff;
-        const float4* gqc = A.qComp + R.sOff;
-        for (int j = lane; j < nS; j += team) {
-            V.q[j] = gq[j];
-            V.omega[j] = gw[j];
-            if (COMP) V.qComp[j] = gqc[j];
-        }
+    teamSync(team, teamIdx);  // the barrier is initialised before anyone polls it
+    if (!mbarWaitBounded(&C.bar, 0, kStageTries)) atomicOr(&C.stageFailed, 1);
+    teamSync(team, teamIdx);  // every lane is past the wait: the barrier can go
+    if (lane == 0) mbarInvalidate(&C.bar);
+    if (C.stageFailed) {  // team-uniform: read after the barrier
+        if (lane == 0 && A.errors) atomicOr(A.errors + r, kErrorStage);
+        fenceProxyAsyncShared();
+        return;
     }
 
     const V3 g{A.gx, A.gy, A.gz};
     const float h = A.h, invH2 = A.invH2;
     const int interval = A.contactInterval;
-    const int* sOrder = A.tOrder + T.sOrderOff;
-    const int* bOrder = A.tOrder + T.bOrderOff;
-    const int* sCol = A.tColorStart + T.sColorOff;
-    const int* bCol = A.tColorStart + T.bColorOff;
     const bool self = R.selfCollision != 0;
     const int table = R.hashTableSize;
 
     const int stepsHere = A.stepsPerLaunch > 0 ? A.stepsPerLaunch : 1;
     for (int step = 0; step < stepsHere; ++step) {
-        if (driveP >= 0 && lane == 0) V.kin[driveP] = driveVelocityB(drive, tRod);
-        if (wayP >= 0 && lane == 0) V.kin[wayP] = waypointVelocity(A.waypoints[r], wayStep + step);
+        if (lane == 0) {
+            if (C.driveP >= 0) V.kin[C.driveP] = driveVelocityB(C.drive, C.tRod);
+            if (C.wayP >= 0) V.kin[C.wayP] = waypointVelocity(A.waypoints[r], C.wayStep + step);
+        }
         teamSync(team, teamIdx);
         for (int sub = 0; sub < A.substeps; ++sub) {
             for (int k = lane; k < nSt; k += team) V.lamS[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -392,7 +561,7 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
                 }
             }
             if (V.numPrims > 0 && maskNow != 0ull) {  // team-uniform; a fully culled world has no slot
-                for (int i = lane; i < nP; i += team) generateSlotsMasked(V, i, regenerate, maskNow);
+                for (int i = lane; i < nP; i += team) generateSlotsMasked<COMP>(V, i, regenerate, maskNow);
             }
             if (self) {
                 if (regenerate) {
@@ -413,76 +582,8 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
                         if (total > R.selfCapacity) *S.overflow += total - R.selfCapacity;
                     }
                     if (live > 0) {
-                        // ---- fill, in the reference's order: its hash buckets ----
-                        for (int t = lane; t <= table; t += team) S.cellStart[t] = 0;
-                        for (int c = lane; c < live; c += team) S.pool[c].seg = -1;
-                        teamSync(team, teamIdx);
-                        for (int j = lane; j < nSt; j += team) {
-                            const float4 c = S.centres[j];
-                            const int h0 = int(hashCell(cellCoord(c.x, cell), cellCoord(c.y, cell),
-                                                        cellCoord(c.z, cell), table));
-                            S.cellOf[j] = h0;
-                            atomicAdd(&S.cellStart[h0], 1);
-                        }
-                        teamSync(team, teamIdx);
-                        // counts -> starts: cellStart[t] = first slot of bucket t,
-                        // cellStart[table] = segment count (the reference's offsets)
-                        teamExclusiveScan(S.cellStart, table + 1, lane, team, teamIdx, partial);
-                        for (int t = lane; t < table; t += team) cursor[t] = S.cellStart[t];
-                        teamSync(team, teamIdx);
-                        // stable placement, one warp walking segments in order
-                        if (lane < 32) {
-                            for (int j0 = 0; j0 < nSt; j0 += 32) {
-                                const int j = j0 + lane;
-                                const bool valid = j < nSt;
-                                const int c = valid ? S.cellOf[j] : -1 - lane;
-                                const unsigned peers = __match_any_sync(0xffffffffu, c);
-                                const int rank = __popc(peers & ((1u << lane) - 1u));
-                                const int start = valid ? cursor[c] : 0;
-                                __syncwarp();
-                                if (valid) {
-                                    S.sorted[start + rank] = j;
-                                    if (rank == 0) cursor[c] = start + __popc(peers);
-                                }
-                                __syncwarp();
-                            }
-                        }
-                        teamSync(team, teamIdx);
-                        for (int j = lane; j < nSt; j += team)
-                            if (S.segCount[j] > 0 && S.segStart[j] < R.selfCapacity)
-                                querySelfSegment<true>(V, S, j, nSt, R.selfGap, table, R.selfCapacity,
-                                                       R.selfFriction, true);
-                        // every thread is done reading the hash (sorted) before
-                        // cellOf and sorted (2 nSt >= nP ints) are reused below
-                        teamSync(team, teamIdx);
-                        for (int i = lane; i < nP; i += team) S.cellOf[i] = 0;
-                        teamSync(team, teamIdx);
-                        if (lane == 0) {
-                            int kept = live;
-                            int n = buildProjectionLevels(S.pool, live, nP, S.cellOf, lvlOf, lvlOrder,
-                                                          lvlStart, &kept);
-                            if (A.precision & kPrecisionColoredSelf) {
-                                // colours instead of levels (the valid prefix is known now)
-                                for (int i = 0; i < nP; ++i) S.cellOf[i] = 0;
-                                const int nc = buildProjectionColors(S.pool, kept, S.cellOf, lvlOf, lvlOrder,
-                                                                     lvlStart);
-                                if (nc >= 0) {
-                                    n = nc;
-                                } else {  // more than 32 colours: keep the levels
-                                    for (int i = 0; i < nP; ++i) S.cellOf[i] = 0;
-                                    n = buildProjectionLevels(S.pool, kept, nP, S.cellOf, lvlOf, lvlOrder,
-                                                              lvlStart, &kept);
-                                }
-                            }
-                            *numLevels = n;
-                            if (kept != live) {
-                                // an entry indexed outside the rod or left unwritten:
-                                // keep the valid prefix and report it, never touch
-                                // memory with it
-                                *S.live = kept;
-                                if (A.errors) atomicOr(A.errors + r, 1);
-                            }
-                        }
+                        fillSelfPool(C, nSt, nP, table, cell, live, R.selfGap, R.selfCapacity, R.selfFriction, A.precision,
+                                     A.errors ? A.errors + r : nullptr, lane, team, teamIdx);
                     } else if (lane == 0) {
                         *numLevels = 0;
                     }
@@ -554,11 +655,7 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
                     // every earlier contact a contact shares a particle with sits in
                     // a lower level -- the serial pool order's result, bit for bit
                     const int nl = *numLevels;
-                    for (int l = 0; l < nl; ++l) {
-                        for (int c = lvlStart[l] + lane; c < lvlStart[l + 1]; c += team)
-                            projectSelf<COMP>(V, S.pool[lvlOrder[c]]);
-                        teamSync(team, teamIdx);
-                    }
+                    if (nl > 0) projectSelfLevels<COMP>(C, nl, lane, team, teamIdx);
                 }
             }
 
@@ -584,27 +681,23 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
                 }
             }
         }
-        tRod += double(A.dt);
+        if (lane == 0) C.tRod += double(A.dt);
     }  // steps of this launch
 
-    // ---- stage out and outputs ----
-    {
-        float4* gx = A.x + R.pOff;
-        float4* gv = A.v + R.pOff;
-        float4* gc = A.xComp + R.pOff;
-        for (int i = lane; i < nP; i += team) {
-            gx[i] = V.x[i];
-            gv[i] = V.v[i];
-            if (COMP) gc[i] = V.xComp[i];
+    // ---- stage out: bulk copies from shared memory, then the outputs ----
+    // every lane's writes above reach the async proxy before lane 0 copies
+    fenceProxyAsyncShared();
+    teamSync(team, teamIdx);
+    if (lane == 0) {
+        bulkStore(A.x + R.pOff, V.x, pBytes);
+        bulkStore(A.v + R.pOff, V.v, pBytes);
+        bulkStore(A.q + R.sOff, V.q, sBytes);
+        bulkStore(A.omega + R.sOff, V.omega, sBytes);
+        if (COMP) {
+            bulkStore(A.xComp + R.pOff, V.xComp, pBytes);
+            bulkStore(A.qComp + R.sOff, V.qComp, sBytes);
         }
-        float4* gq = A.q + R.sOff;
-        float4* gw = A.omega + R.sOff;
-        float4* gqc = A.qComp + R.sOff;
-        for (int j = lane; j < nS; j += team) {
-            gq[j] = V.q[j];
-            gw[j] = V.omega[j];
-            if (COMP) gqc[j] = V.qComp[j];
-        }
+        bulkCommit();
     }
     if (V.numPrims > 0 && A.contactState) {
         const int slots = nP * V.numPrims;
@@ -617,9 +710,13 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
     }
     if (lane == 0) {
         if (self) A.selfCount[r] = *S.live;
-        A.rodTime[r] = tRod;
-        if (wayP >= 0) A.waypoints[r].step = wayStep + stepsHere;
+        A.rodTime[r] = C.tRod;
+        if (C.wayP >= 0) A.waypoints[r].step = C.wayStep + stepsHere;
     }
+    // the stores have read the rows, and every lane's accesses of this shared
+    // memory come before the next rod's bulk copies overwrite it
+    if (lane == 0) bulkWaitRead();
+    fenceProxyAsyncShared();
 }
 
 template <bool COMP, bool FP64>
@@ -627,6 +724,7 @@ __global__ void __launch_bounds__(256, 2) kBatchedStep(DArgs A, const int32_t* _
                                                        int numGroups, int32_t* queue) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int sGroup;
+    __shared__ TeamCtx ctxs[kMaxTeamsPerCta];
     const int tid = threadIdx.x;
     for (;;) {
         if (tid == 0) sGroup = atomicAdd(queue, 1);
@@ -646,10 +744,11 @@ __global__ void __launch_bounds__(256, 2) kBatchedStep(DArgs A, const int32_t* _
                                         Rk.hashTableSize, Rk.selfCapacity, 1, COMP ? 1 : 0, A.slotsShared)
                                   .bytes);
             }
-            runRod<COMP, FP64>(A, A.work[first + teamIdx], smem + off, lane, team, teamIdx);
+            runRod<COMP, FP64>(A, A.work[first + teamIdx], smem + off, lane, team, teamIdx, ctxs);
         }
         __syncthreads();
     }
+    bulkWaitAll();  // this thread's state stores are complete before it exits
     // The last CTA out resets the queue for the next launch.
     if (tid == 0) {
         __threadfence();
@@ -706,6 +805,19 @@ cudaError_t batchedReserveSmem(size_t bytes) {
     e = setMaxDynamicSmem_batched(want);
     if (e == cudaSuccess) reserved[dev] = want;
     return e;
+}
+
+// The kernel's static shared memory (team contexts, the group word): the
+// dynamic part of a plan may use the opt-in limit minus this.
+size_t batchedStaticSmem() {
+    size_t most = 0;
+    cudaFuncAttributes a;
+    if (cudaFuncGetAttributes(&a, kBatchedStep<false, false>) == cudaSuccess) most = std::max(most, a.sharedSizeBytes);
+    if (cudaFuncGetAttributes(&a, kBatchedStep<false, true>) == cudaSuccess) most = std::max(most, a.sharedSizeBytes);
+    if (cudaFuncGetAttributes(&a, kBatchedStep<true, false>) == cudaSuccess) most = std::max(most, a.sharedSizeBytes);
+    if (cudaFuncGetAttributes(&a, kBatchedStep<true, true>) == cudaSuccess) most = std::max(most, a.sharedSizeBytes);
+    cudaGetLastError();
+    return most;
 }
 
 cudaError_t batchedOccupancy(int threads, size_t smem, int precision, int* perSm) {

@@ -26,6 +26,9 @@ struct BatchedPlan {
 cudaError_t launchBatchedStep(const DArgs& a, const BatchedPlan& plan, int precision,
                               cudaStream_t stream);
 cudaError_t batchedReserveSmem(size_t bytes);
+// Static shared memory of the batched kernel (bytes), which a plan's dynamic
+// shared memory must leave room for under the opt-in limit.
+size_t batchedStaticSmem();
 cudaError_t batchedOccupancy(int threads, size_t smemBytes, int precision, int* blocksPerSm);
 
 // Address and size of this device's static scratch array (looked up on the

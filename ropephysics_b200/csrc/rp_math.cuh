@@ -220,6 +220,79 @@ __device__ __forceinline__ float signedDistance(const PrimF& P, V3 p, V3& n) {
     return -depth;
 }
 
+// The same signed distance in FP64, at a position given in double: the
+// compensated contact constraint needs the gap to better than the FP32
+// spacing of the position itself (a particle 1 m from the origin is only
+// known to 6e-8 m in FP32, about one substep's contact penetration under
+// gravity). The primitive keeps its FP32 data (a fixed shift of the surface,
+// the same every substep); the normal is rounded to FP32.
+struct D3 {
+    double x, y, z;
+};
+__device__ __forceinline__ D3 dsub(D3 a, D3 b) { return D3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ D3 dadd(D3 a, D3 b) { return D3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ D3 dscale(D3 a, double s) { return D3{a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ double ddot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ D3 dcross(D3 a, D3 b) {
+    return D3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ D3 dof(V3 v) { return D3{double(v.x), double(v.y), double(v.z)}; }
+__device__ __forceinline__ V3 fof(D3 v) { return V3{float(v.x), float(v.y), float(v.z)}; }
+// v rotated by the unit quaternion (w, u): v + 2w (u x v) + 2 u x (u x v)
+__device__ __forceinline__ D3 drotate(double w, D3 u, D3 v) {
+    const D3 t = dscale(dcross(u, v), 2.0);
+    return dadd(dadd(v, dscale(t, w)), dcross(u, t));
+}
+__device__ __forceinline__ double distanceToSphereLikeD(D3 centre, float radius, D3 p, V3& n) {
+    const D3 d = dsub(p, centre);
+    const double len = sqrt(ddot(d, d));
+    n = len > 1e-12 ? fof(dscale(d, 1.0 / len)) : V3{0.0f, 0.0f, 1.0f};
+    return len - double(radius);
+}
+__device__ __forceinline__ double signedDistanceD(const PrimF& P, D3 p, V3& n) {
+    const D3 a = dof(P.a);
+    if (P.type == 0) {
+        n = P.n;
+        return ddot(dsub(p, a), dof(P.n));
+    }
+    if (P.type == 1) return distanceToSphereLikeD(a, P.radius, p, n);
+    if (P.type == 2) {
+        const D3 ab = dsub(dof(P.b), a);
+        const double len2 = ddot(ab, ab);
+        double t = len2 < 1e-30 ? 0.0 : ddot(dsub(p, a), ab) / len2;
+        t = t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t);
+        return distanceToSphereLikeD(dadd(a, dscale(ab, t)), P.radius, p, n);
+    }
+    // box: the point in the box frame (conjugate rotation), clamped to the extents
+    const D3 u{double(P.rot.x), double(P.rot.y), double(P.rot.z)};
+    const D3 local = drotate(double(P.rot.w), D3{-u.x, -u.y, -u.z}, dsub(p, a));
+    const double hx = P.h.x, hy = P.h.y, hz = P.h.z;
+    const D3 clamped{local.x < -hx ? -hx : (local.x > hx ? hx : local.x),
+                     local.y < -hy ? -hy : (local.y > hy ? hy : local.y),
+                     local.z < -hz ? -hz : (local.z > hz ? hz : local.z)};
+    const D3 delta = dsub(local, clamped);
+    const double outside = sqrt(ddot(delta, delta));
+    if (outside > 1e-12) {
+        n = fof(drotate(double(P.rot.w), u, dscale(delta, 1.0 / outside)));
+        return outside;
+    }
+    const double dx = hx - fabs(local.x), dy = hy - fabs(local.y), dz = hz - fabs(local.z);
+    D3 nn;
+    double depth;
+    if (dx <= dy && dx <= dz) {
+        nn = D3{local.x >= 0.0 ? 1.0 : -1.0, 0.0, 0.0};
+        depth = dx;
+    } else if (dy <= dz) {
+        nn = D3{0.0, local.y >= 0.0 ? 1.0 : -1.0, 0.0};
+        depth = dy;
+    } else {
+        nn = D3{0.0, 0.0, local.z >= 0.0 ? 1.0 : -1.0};
+        depth = dz;
+    }
+    n = fof(drotate(double(P.rot.w), u, nn));
+    return -depth;
+}
+
 // Closest points between segments [p1,q1] and [p2,q2] as parameters s, t.
 __device__ __forceinline__ void closestPointsBetweenSegments(V3 p1, V3 q1, V3 p2, V3 q2, float& s,
                                                              float& t) {

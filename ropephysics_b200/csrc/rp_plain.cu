@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(128, 4) kPlainStep(DArgs A) {
         for (int k = tid; k < nB; k += nth) V.lamB[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         const bool regenerate = sub % interval == 0;
         if (V.numPrims > 0)
-            for (int i = tid; i < nP; i += nth) generateSlots(V, i, regenerate);
+            for (int i = tid; i < nP; i += nth) generateSlots<COMP>(V, i, regenerate);
         if (self) {
             if (regenerate) {
                 if (tid == 0) {

@@ -310,7 +310,7 @@ bool rp_server::plan() {
     for (auto& rq : running) ids.insert(ids.end(), rq->rodIds.begin(), rq->rodIds.end());
     const bool comp = (cfg.precision & RP_PRECISION_COMPENSATED) != 0;
     smem = rpx::planGroups(ids, hRods.data(), hTmpls.data(), 256, 1, comp, order, groups);
-    if (smem + 1024 > rpx::optinSmem(device)) {
+    if (smem + rp::batchedStaticSmem() + 64 > rpx::optinSmem(device)) {
         workerError = "a rod group exceeds shared memory";
         return false;
     }

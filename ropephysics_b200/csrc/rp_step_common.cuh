@@ -225,32 +225,61 @@ __device__ __forceinline__ void projectBendOne(const RodView& V, int k, float in
 
 // ---------------------------------------------------------------- world contacts
 
+// One slot of particle i against primitive P, from its start-of-substep
+// position. Reference order: the reference's FP32 gap and offset = x . n -
+// gap. Compensated: the gap is evaluated in FP64 at the true position
+// x - xComp and kept as the slot's offset, and the constraint is then
+// measured from the substep's displacement accumulator (projectSlots), so no
+// rounding of a position near 1 m enters C.
+template <bool COMP>
+__device__ __forceinline__ void generateSlot(const RodView& V, int i, const PrimF& P, DSlot& c) {
+    V3 n;
+    if (!COMP) {
+        const V3 x = v3(V.x[i]);
+        const float gap = signedDistance(P, x, n) - V.radius;
+        if (gap >= V.contactMargin) return;
+        c.offset = dot(x, n) - gap;
+    } else {
+        const float4 xs = V.x[i], cs = V.xComp[i];
+        const D3 xt{double(xs.x) - double(cs.x), double(xs.y) - double(cs.y), double(xs.z) - double(cs.z)};
+        const double gap = signedDistanceD(P, xt, n) - double(V.radius);
+        if (gap >= double(V.contactMargin)) return;
+        c.offset = float(gap);
+    }
+    c.state = 1;
+    c.nx = n.x;
+    c.ny = n.y;
+    c.nz = n.z;
+    c.friction = P.friction * V.frictionScale;
+}
+
+// A kept slot between regenerations: its multipliers restart. Compensated,
+// its gap moves to the start of this substep by the previous substep's
+// displacement (still in the accumulator: the prediction resets it after
+// the slots are handled).
+template <bool COMP>
+__device__ __forceinline__ void keepSlot(const RodView& V, int i, DSlot& c) {
+    if (COMP && c.state != 0) c.offset += dot(v3(V.xPrev[i]), V3{c.nx, c.ny, c.nz});
+    c.state = c.state != 0 ? 1 : 0;
+}
+
 // Rebuild particle i's slots from its start-of-substep position, or between
 // regenerations only reset their multipliers.
+template <bool COMP>
 __device__ __forceinline__ void generateSlots(const RodView& V, int i, bool regenerate) {
     const int base = i * V.numPrims;
     const float w = V.invMass[i];
-    const V3 x = v3(V.x[i]);
     for (int k = 0; k < V.numPrims; ++k) {
         DSlot& c = V.slots[base + k];
         c.lambdaN = 0.0f;
         c.applied = 0.0f;
         if (!regenerate) {
-            c.state = c.state != 0 ? 1 : 0;
+            keepSlot<COMP>(V, i, c);
             continue;
         }
         c.state = 0;
         if (w == 0.0f) continue;  // pinned: cannot respond
-        const PrimF P = loadPrim(V.prims[k]);
-        V3 n;
-        const float gap = signedDistance(P, x, n) - V.radius;
-        if (gap >= V.contactMargin) continue;
-        c.state = 1;
-        c.nx = n.x;
-        c.ny = n.y;
-        c.nz = n.z;
-        c.offset = dot(x, n) - gap;
-        c.friction = P.friction * V.frictionScale;
+        generateSlot<COMP>(V, i, loadPrim(V.prims[k]), c);
     }
 }
 
@@ -296,32 +325,23 @@ __device__ __forceinline__ unsigned long long primitivesNearBox(const RodView& V
 // generateSlots for the primitives in `mask`. The slots of the others are not
 // touched: they hold no contact, and every reader (projection, the state
 // output) consults the same mask.
+template <bool COMP>
 __device__ __forceinline__ void generateSlotsMasked(const RodView& V, int i, bool regenerate,
                                                     unsigned long long mask) {
     const int base = i * V.numPrims;
     const float w = V.invMass[i];
-    const V3 x = v3(V.x[i]);
     for (int k = 0; k < V.numPrims; ++k) {
         if (!((mask >> k) & 1ull)) continue;
         DSlot& c = V.slots[base + k];
         c.lambdaN = 0.0f;
         c.applied = 0.0f;
         if (!regenerate) {
-            c.state = c.state != 0 ? 1 : 0;
+            keepSlot<COMP>(V, i, c);
             continue;
         }
         c.state = 0;
         if (w == 0.0f) continue;
-        const PrimF P = loadPrim(V.prims[k]);
-        V3 n;
-        const float gap = signedDistance(P, x, n) - V.radius;
-        if (gap >= V.contactMargin) continue;
-        c.state = 1;
-        c.nx = n.x;
-        c.ny = n.y;
-        c.nz = n.z;
-        c.offset = dot(x, n) - gap;
-        c.friction = P.friction * V.frictionScale;
+        generateSlot<COMP>(V, i, loadPrim(V.prims[k]), c);
     }
 }
 
@@ -339,7 +359,8 @@ __device__ __forceinline__ void projectSlots(const RodView& V, int i, unsigned l
         if (!c.state) continue;
         const V3 n{c.nx, c.ny, c.nz};
 
-        const float C = dot(v3(V.x[i]), n) - c.offset;
+        // compensated: the gap at the substep's start plus the displacement since
+        const float C = COMP ? dot(dispOf<COMP>(V, i), n) + c.offset : dot(v3(V.x[i]), n) - c.offset;
         float dLambda = -C / w;
         const float clamped = c.lambdaN + dLambda > 0.0f ? c.lambdaN + dLambda : 0.0f;
         dLambda = clamped - c.lambdaN;

@@ -134,6 +134,16 @@ def uneven(num_rods: int = 16384, seed: int = 0, min_seg: int = 16, max_seg: int
     return out
 
 
+def shard(draws: List[UnevenRod], k: int, n: int) -> List[UnevenRod]:
+    """The k-th of n shards of a batch: rods sorted by length (stable), every
+    n-th from position k, so each shard holds the same spread of lengths and
+    the shards of one batch are disjoint and cover it. No rod of one shard
+    interacts with another's (rods are independent), so shards step on
+    separate GPUs with no exchange."""
+    order = sorted(range(len(draws)), key=lambda i: -draws[i].segments)
+    return [draws[i] for i in order[k::n]]
+
+
 @dataclass
 class GridDraws:
     youngs_scale: np.ndarray  # float32, per rod

@@ -105,17 +105,22 @@ def _random_primitive(rng, centre, mu, lo, hi, clearance=0.02, tries=64) -> Prim
 
 
 def uneven(num_rods: int = 16384, seed: int = 0, min_seg: int = 16, max_seg: int = 512,
-           substeps: int = 50, hash_table_size: int = 0) -> Workload:
+           substeps: int = 50, hash_table_size: int = 0, shard=None) -> Workload:
     """Uneven batch: rods of 16..512 segments, coiled, each with its own world.
-    hash_table_size 0 sizes each rod's table with table_for()."""
+    hash_table_size 0 sizes each rod's table with table_for(). shard=(k, n):
+    the k-th of n shards of a batch of n x num_rods rods drawn from `seed`
+    (synth.shard: length-sorted, every n-th rod)."""
     rods, worlds = [], []
-    for d in synth.uneven(num_rods, seed, min_seg, max_seg, hash_table_size):
+    draws = synth.uneven(num_rods * (shard[1] if shard else 1), seed, min_seg, max_seg, hash_table_size)
+    if shard:
+        draws = synth.shard(draws, *shard)
+    for d in draws:
         rod = Rod.centerline(d.points, GRID_MATERIAL, frame_seed=(0.0, 0.0, 1.0))
         rod.b_rest_darboux[:] = 0.0  # straight rest shape: the coil is loaded
         rods.append(rod)
         worlds.append(World([primitive(q) for q in d.prims], self_collision=True, self_friction=d.friction,
                             hash_table_size=d.hash_table_size))
-    return Workload(f"uneven-{num_rods}x[{min_seg},{max_seg}]", rods, worlds, list(range(num_rods)),
+    return Workload(f"uneven-{len(rods)}x[{min_seg},{max_seg}]", rods, worlds, list(range(len(rods))),
                     StepParams(dt=1.0 / 60, substeps=substeps, iterations=1), steps=500,
                     info=dict(seed=seed, hash_table_size=hash_table_size or "2n, pow2, 64..1024"))
 

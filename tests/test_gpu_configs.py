@@ -1,0 +1,465 @@
+"""Parity on the benchmark configurations against the reference's own FP32
+GPU path and its FP64 CPU solver.
+
+The reference's CUDA batch (src/gpu/gpu_solver.cu + gpu_batch.cpp, compiled
+for sm_100a into oracle/_ref/libcrs_ref_gpu.so) runs each configuration it
+can express beside this library on the same B200, following the reference's
+own methodology (src/gpu/gpu_cases.cpp): checkpoints after 1, 10, 50 and 200
+steps (:165-169), and restart comparisons (:421-546) -- the reference's state
+at a restart point is loaded into this library, and both then step from the
+identical state. Tolerance: 1e-5 of the rod length in position and 1e-5 in
+quaternion components, for the 10 steps after each restart. Beyond that the
+two FP32 paths part like the reference's own float-vs-double drift (contact
+and self-contact decisions at ulp distance), so free-running drift is
+printed, not asserted tightly.
+
+  config 1  the 64-segment cantilever (E 1e8, tip load 0.05 N, dt 1/60, 20
+            substeps) for the full 2000 steps: tip deflection and centre line
+            against the FP64 CPU oracle and against the reference GPU kernel
+  config 2  the 4096 x 64 driven grid in one reference batch (per-rod
+            stiffness and friction scales, floor, kinematic top uploaded every
+            step as the reference's API does), restarts after 0, 100 and 500
+            steps
+  config 3  24 rods sampled from the uneven batch, each with its own world
+            (1-4 primitives, self-collision), each in its own reference batch;
+            restarts after 0, 100 and 500 steps, and at every restart point
+            the self-contact pair lists and world-contact active sets of one
+            substep bit-exact against the reference kernel
+"""
+import ctypes as C
+import math
+
+import numpy as np
+import pytest
+
+import ropephysics_b200 as rp
+from oracle import Primitive as OP, World as OW
+from ropephysics_b200 import synth
+from ropephysics_b200 import workloads as W
+from tests.helpers import max_dq, max_dx, oparams, product_rod
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+WINDOW = 10
+RESTARTS = (0, 100, 500)
+FP = C.POINTER(C.c_float)
+MIXED = int(rp.Precision.COMPENSATED | rp.Precision.FP64_CONE | rp.Precision.FP64_VERDICT)
+
+
+def _need(R):
+    if not R.lib.refgpu_available():
+        pytest.skip("no device for the reference GPU path")
+
+
+def _gravity(p):
+    return (C.c_double * 3)(*p.gravity)
+
+
+def _load_state(batch, rod_index, proto, x, v, q, w):
+    """The reference's float state of one rod into this library's batch."""
+    proto.x[...] = x
+    proto.v[...] = v
+    proto.q[...] = q
+    proto.omega[...] = w
+    batch.upload_rod(rod_index, proto)
+
+
+# ----------------------------------------------------------------------------- config 1
+
+
+def test_cantilever_2000_steps(reference_gpu, oracle64):
+    R = reference_gpu
+    _need(R)
+    o = oracle64.straight(64, 1.0, youngs=1e8, poisson=0.3, density=1100.0, radius=5e-3)
+    oracle64.clamp(o, False)
+    o.extForce[o.nP - 1] = (0.0, 0.0, -0.05)
+    proto = product_rod(o)
+    p = rp.StepParams(dt=1.0 / 60, substeps=20, iterations=1)
+    ours = {}
+    for name, strat, prec in (("batched", rp.Strategy.BATCHED, 0), ("fused", rp.Strategy.FUSED, 0),
+                              ("mixed", rp.Strategy.BATCHED, MIXED)):
+        b = rp.Batch.create(proto, 1, strat)
+        b.set_precision(prec)
+        ours[name] = b
+    h = R.from_rod(o)
+    rb = R.lib.refgpu_create(h, 1, 1, None)
+    assert rb
+    g = _gravity(p)
+    op = oparams(p)
+    done = 0
+    rows = []
+    for cp in (1, 10, 50, 200, 2000):
+        k = cp - done
+        R.lib.refgpu_step(rb, p.dt, p.substeps, p.iterations, g, 0.0, 0.0, 1, k)
+        for b in ours.values():
+            b.step_many(p, k)
+        oracle64.step(o, op, steps=k)
+        done = cp
+        R.lib.refgpu_sync(rb)
+        rx, _, rq, _ = R.gpu_state(rb, 1, o.nP, o.nS)
+        fx = o.x[: o.nP]
+        row = {"step": cp, "tip_fp64": fx[-1, 2], "tip_refgpu": float(rx[0, -1, 2])}
+        for name, b in ours.items():
+            x, q = b.download_positions(), b.download_frames()
+            row[f"tip_{name}"] = float(x[-1, 2])
+            row[f"{name}_vs_refgpu"] = (max_dx(x, rx[0]), max_dq(q, rq[0]))
+            row[f"{name}_vs_fp64"] = max_dx(x, fx)
+        row["refgpu_vs_fp64"] = max_dx(rx[0], fx)
+        rows.append(row)
+    for r in rows:
+        print(f"\ncantilever step {r['step']}: tip z FP64 {r['tip_fp64']:.6f} reference GPU {r['tip_refgpu']:.6f} "
+              f"ours {r['tip_batched']:.6f} mixed {r['tip_mixed']:.6f}; max centre-line error vs FP64: "
+              f"reference GPU {r['refgpu_vs_fp64']:.2e}, ours {r['batched_vs_fp64']:.2e}, "
+              f"mixed {r['mixed_vs_fp64']:.2e}; ours vs reference GPU dx {r['batched_vs_refgpu'][0]:.2e} "
+              f"dq {r['batched_vs_refgpu'][1]:.2e}")
+    for r in rows:
+        # the reference-order paths follow the reference kernel
+        for name in ("batched", "fused"):
+            dx, dq = r[f"{name}_vs_refgpu"]
+            assert dx <= TOL * 1.0 and dq <= TOL, (r["step"], name, dx, dq)
+        # mixed precision stays on the FP64 solution
+        assert r["mixed_vs_fp64"] <= 1e-6, r
+    # the large-deflection load really bends it (rho A g L^3 / EI ~ 17)
+    assert rows[-1]["tip_fp64"] < -0.3
+    R.lib.refgpu_free(rb)
+    R.free(h)
+    for b in ours.values():
+        b.close()
+
+
+# ----------------------------------------------------------------------------- config 2
+
+
+def drive_velocities(wl, t):
+    """Kinematic velocity of every particle at time t, rod-major float32: the
+    pinned top moves along z at A 2 pi f cos(2 pi f t + phase)."""
+    n_rods, n_p = len(wl.rods), wl.rods[0].num_particles
+    v = np.zeros((n_rods, n_p, 3), np.float32)
+    for r, d in enumerate(wl.drives):
+        w = 2 * math.pi * d.frequency
+        v[r, d.particle, 2] = d.amplitude * w * math.cos(w * t + d.phase)
+    return v.reshape(-1)
+
+
+def test_grid_restarts_vs_reference_gpu(reference_gpu, oracle64):
+    R = reference_gpu
+    _need(R)
+    wl = W.grid(4096)
+    n_rods, p = len(wl.rods), wl.params
+    o = oracle64.straight(64, 1.0, youngs=1e8, poisson=0.3, density=1100.0, radius=5e-3, direction=(0, 0, -1))
+    oracle64.pin(o, 0)
+    h = R.from_rod(o)
+    rb = R.lib.refgpu_create(h, n_rods, 1, R.world(OW([OP.plane((0, 0, -1.2), (0, 0, 1), 0.5)])))
+    assert rb
+    ys = np.ascontiguousarray(wl.youngs_scale, np.float32)
+    fs = np.ascontiguousarray(wl.friction_scale, np.float32)
+    R.lib.refgpu_set_material_scales(rb, ys.ctypes.data_as(FP), fs.ctypes.data_as(FP), n_rods)
+    proto = product_rod(o)
+    world = rp.World([rp.Primitive.plane((0, 0, -1.2), (0, 0, 1), 0.5)])
+    free = rp.Batch.create(proto, n_rods, rp.Strategy.BATCHED, world)
+    rest = rp.Batch.create(proto, n_rods, rp.Strategy.BATCHED, world)
+    for b in (free, rest):
+        b.set_material_scales(ys, fs)
+    g = _gravity(p)
+    nP, nS = o.nP, o.nS
+    drift, worst = {}, {}
+    s, window_end, start = 0, -1, None
+    while s < RESTARTS[-1] + WINDOW:
+        if s in RESTARTS:
+            R.lib.refgpu_sync(rb)
+            x, v, q, w = R.gpu_state(rb, n_rods, nP, nS)
+            for r in range(n_rods):
+                _load_state(rest, r, proto, x[r], v[r], q[r], w[r])
+            start, window_end = s, s + WINDOW
+        kv = drive_velocities(wl, s * p.dt)
+        R.lib.refgpu_set_kinematic(rb, kv.ctypes.data_as(FP), len(kv) // 3)
+        R.lib.refgpu_step(rb, p.dt, p.substeps, p.iterations, g, 0.0, 0.0, 1, 1)
+        if s < 200:
+            free.set_kinematic_velocities(kv)
+            free.step(p)
+        if s < window_end:
+            rest.set_kinematic_velocities(kv)
+            rest.step(p)
+        s += 1
+        if s in (1, 10, 50, 200) or s <= window_end:
+            R.lib.refgpu_sync(rb)
+            rx, _, rq, _ = R.gpu_state(rb, n_rods, nP, nS)
+            if s in (1, 10, 50, 200):
+                drift[s] = max_dx(free.download_positions(), rx)
+            if s <= window_end:
+                dx = max_dx(rest.download_positions(), rx)
+                dq = max_dq(rest.download_frames(), rq) if (s - start) in (1, 5, WINDOW) else 0.0
+                a = worst.setdefault(start, [0.0, 0.0])
+                a[0], a[1] = max(a[0], dx), max(a[1], dq)
+    print(f"\ngrid 4096x64 vs the reference GPU batch: restart windows (max over {WINDOW} steps) "
+          + ", ".join(f"after {k}: dx {v[0]:.2e} dq {v[1]:.2e}" for k, v in worst.items())
+          + "; free-running drift " + ", ".join(f"{k}: {v:.2e}" for k, v in drift.items()))
+    for k, (dx, dq) in worst.items():
+        assert dx <= TOL * 1.0 and dq <= TOL, (k, dx, dq)
+    assert drift[10] <= TOL
+    R.lib.refgpu_free(rb)
+    R.free(h)
+    free.close()
+    rest.close()
+
+
+# ----------------------------------------------------------------------------- config 3
+
+
+def _one_substep(p):
+    return rp.StepParams(dt=float(np.float32(p.dt)) / p.substeps, substeps=1, iterations=p.iterations,
+                         gravity=p.gravity)
+
+
+def test_uneven_sample_restarts_vs_reference_gpu(reference_gpu):
+    R = reference_gpu
+    _need(R)
+    draws = synth.uneven(16384, 0)
+    idx = np.random.default_rng(7).choice(len(draws), size=24, replace=False)
+    mat = dict(youngs=synth.YOUNGS, poisson=synth.POISSON, density=synth.DENSITY, radius=synth.RADIUS)
+    p = rp.StepParams(dt=1.0 / 60, substeps=50, iterations=1)
+    one = _one_substep(p)
+    g, g1 = _gravity(p), _gravity(one)
+    refs, protos, worlds, owlds = [], [], [], []
+    for i in idx:
+        d = draws[i]
+        h = R.centerline(d.points, frame_seed=(0.0, 0.0, 1.0), **mat)
+        rr = R.export(h)
+        rr.bRestD[:] = 0.0
+        R.import_state(h, rr)
+        ow = OW([OP(*q) for q in d.prims], True, d.friction, 2, d.hash_table_size, 0.25)
+        wh = R.world(ow)
+        rb = R.lib.refgpu_create(h, 1, 1, wh) or R.lib.refgpu_create(h, 1, 0, wh)  # fused if it fits
+        assert rb
+        refs.append((h, wh, rb, rr.nP, rr.nS, 0.2 * d.segments / 32))
+        protos.append(product_rod(rr))
+        owlds.append(ow)
+        worlds.append(rp.World([W.primitive(q) for q in d.prims], self_collision=True, self_friction=d.friction,
+                               hash_table_size=d.hash_table_size))
+    n = len(idx)
+    rest = rp.Batch.create_mixed(protos, worlds, list(range(n)), rp.Strategy.BATCHED)
+    worst, pairs_total, active_total = {}, 0, 0
+    s = 0
+    for start in RESTARTS:
+        for h, wh, rb, *_ in refs:
+            R.lib.refgpu_step(rb, p.dt, p.substeps, p.iterations, g, 0.0, 0.0, 1, start - s)
+        s = start
+        states = []
+        for r, (h, wh, rb, nP, nS, _) in enumerate(refs):
+            R.lib.refgpu_sync(rb)
+            x, v, q, w = R.gpu_state(rb, 1, nP, nS)
+            states.append((x[0], v[0], q[0], w[0]))
+            _load_state(rest, r, protos[r], x[0], v[0], q[0], w[0])
+            # one substep from this state: pair lists and active sets exact
+            # against the reference's multi-kernel path (its global pool)
+            st = R.export(h)
+            st.x[:nP], st.v[:nP], st.q[:nS], st.omega[:nS] = x[0], v[0], q[0], w[0]
+            h1 = R.from_rod(st)
+            rb1 = R.lib.refgpu_create(h1, 1, 0, wh)
+            assert rb1
+            R.lib.refgpu_step(rb1, one.dt, 1, one.iterations, g1, 0.0, 0.0, 1, 1)
+            R.lib.refgpu_sync(rb1)
+            expect_pairs = R.gpu_self_pairs(rb1)
+            prims = len(owlds[r].primitives)
+            expect_active = R.gpu_contact_active(rb1, 0, nP, prims)
+            b1 = rp.Batch.create(protos[r], 1, rp.Strategy.BATCHED, worlds[r])
+            b1.step(one)
+            got_pairs = [tuple(int(t) for t in pr) for pr in b1.read_self_contacts(0)]
+            got_active = (b1.read_contact_states().reshape(nP, prims) != 0).astype(np.int32)
+            assert got_pairs == expect_pairs, (start, r, len(got_pairs), len(expect_pairs))
+            assert np.array_equal(got_active, expect_active), (start, r)
+            pairs_total += len(expect_pairs)
+            active_total += int(expect_active.sum())
+            b1.close()
+            R.lib.refgpu_free(rb1)
+            R.free(h1)
+        for k in range(1, WINDOW + 1):
+            rest.step(p)
+            xs, qs = rest.download_positions(), rest.download_frames()
+            for r, (h, wh, rb, nP, nS, length) in enumerate(refs):
+                R.lib.refgpu_step(rb, p.dt, p.substeps, p.iterations, g, 0.0, 0.0, 1, 1)
+                R.lib.refgpu_sync(rb)
+                rx, _, rq, _ = R.gpu_state(rb, 1, nP, nS)
+                dx = max_dx(rest.positions_of(r, xs), rx[0]) / length
+                dq = max_dq(rest.frames_of(r, qs), rq[0])
+                a = worst.setdefault(start, [0.0, 0.0])
+                a[0], a[1] = max(a[0], dx), max(a[1], dq)
+        s = start + WINDOW
+    print(f"\nuneven sample of {n} rods vs the reference GPU kernel: restart windows (max over {WINDOW} steps, "
+          "dx relative to the rod length) "
+          + ", ".join(f"after {k}: dx {v[0]:.2e} dq {v[1]:.2e}" for k, v in worst.items())
+          + f"; {pairs_total} self-contact pairs and {active_total} active world contacts bit-exact")
+    for k, (dx, dq) in worst.items():
+        assert dx <= TOL and dq <= TOL, (k, dx, dq)
+    assert pairs_total > 0 and active_total > 0
+    assert rest.error_count() == 0
+    rest.close()
+    for h, wh, rb, *_ in refs:
+        R.lib.refgpu_free(rb)
+        R.free(h)
+
+
+# ----------------------------------------------------------------------------- error vs FP64
+
+
+def _run_three(R, orods, oworlds, op, protos, worlds, p, checkpoints, kin=None, scales=None, ref_worlds=None):
+    """Step the same rods on the FP64 oracle, on this library in reference
+    order and in mixed precision, and on the reference GPU kernel (one batch
+    per rod); max |dx| against FP64 (relative to each rod's length) at every
+    checkpoint. kin(s) -> per-rod kinematic velocity of particle 0 at step s."""
+    from oracle import Oracle, Context
+    o64 = Oracle("f64")
+    n = len(orods)
+    ours = {}
+    for name, prec in (("reference order", 0), ("mixed", MIXED)):
+        b = rp.Batch.create_mixed(protos, worlds, list(range(n)), rp.Strategy.BATCHED)
+        b.set_precision(prec)
+        if scales is not None:
+            b.set_material_scales(*scales)
+        ours[name] = b
+    refs = []
+    g = _gravity(p)
+    for r in range(n):
+        h = R.from_rod(orods[r])
+        rw = (ref_worlds or oworlds)[r]
+        wh = R.world(rw) if rw is not None else None
+        rb = R.lib.refgpu_create(h, 1, 1, wh) or R.lib.refgpu_create(h, 1, 0, wh)
+        assert rb
+        if scales is not None:
+            ys = np.ascontiguousarray(scales[0][r:r + 1], np.float32)
+            fs = np.ascontiguousarray(scales[1][r:r + 1], np.float32)
+            R.lib.refgpu_set_material_scales(rb, ys.ctypes.data_as(FP), fs.ctypes.data_as(FP), 1)
+        refs.append((h, rb))
+    if scales is not None:
+        # the FP64 rods carry the stiffness scale in their compliance (the
+        # reference's own note: compliance x 1 / scale equals building the rod
+        # with that modulus); friction scales are in their worlds already
+        for r, o in enumerate(orods):
+            o.sComp[: o.nSt] /= float(scales[0][r])
+            o.bComp[: o.nB] /= float(scales[0][r])
+    ctxs = [Context(dtype=np.float64) if w is not None else None for w in oworlds]
+    lengths = [float(np.sum(np.linalg.norm(np.diff(o.x[: o.nP], axis=0), axis=1))) for o in orods]
+    rows, done = {}, 0
+    for cp in checkpoints:
+        for s in range(done, cp):
+            if kin is not None:
+                v = kin(s)  # (rods, 3)
+                for r, o in enumerate(orods):
+                    o.kinVel[0] = v[r].astype(np.float32).astype(np.float64)
+                    kv = np.zeros((o.nP, 3), np.float32)
+                    kv[0] = v[r]
+                    R.lib.refgpu_set_kinematic(refs[r][1], kv.ctypes.data_as(FP), o.nP)
+                kv_all = np.concatenate([np.vstack([v[r][None], np.zeros((o.nP - 1, 3))])
+                                         for r, o in enumerate(orods)]).astype(np.float32)
+                for b in ours.values():
+                    b.set_kinematic_velocities(kv_all)
+            for r, o in enumerate(orods):
+                o64.step(o, op, world=oworlds[r], ctx=ctxs[r])
+                R.lib.refgpu_step(refs[r][1], p.dt, p.substeps, p.iterations, g, 0.0, 0.0, 1, 1)
+            for b in ours.values():
+                b.step(p)
+        done = cp
+        row = {}
+        for name, b in ours.items():
+            x = b.download_positions()
+            row[name] = max(max_dx(b.positions_of(r, x), o.x[: o.nP]) / lengths[r] for r, o in enumerate(orods))
+        worst = 0.0
+        for r, o in enumerate(orods):
+            R.lib.refgpu_sync(refs[r][1])
+            rx, _, _, _ = R.gpu_state(refs[r][1], 1, o.nP, o.nS)
+            worst = max(worst, max_dx(rx[0], o.x[: o.nP]) / lengths[r])
+        row["reference GPU"] = worst
+        rows[cp] = row
+    for b in ours.values():
+        b.close()
+    for h, rb in refs:
+        R.lib.refgpu_free(rb)
+        R.free(h)
+    return rows
+
+
+def _print_rows(name, rows):
+    for cp, row in rows.items():
+        print(f"\n{name} step {cp}: max |dx| / L vs FP64: " + ", ".join(f"{k} {v:.2e}" for k, v in row.items()))
+
+
+def test_error_vs_fp64_grid(reference_gpu, oracle64):
+    """Config 2, 8 rods spread over the grid's draws, 1000 steps (the
+    config's horizon) with the drive's kinematic velocity uploaded per step."""
+    R = reference_gpu
+    _need(R)
+    wl = W.grid(4096)
+    pick = list(range(0, 4096, 512))
+    p = wl.params
+    orods, oworlds, protos, worlds = [], [], [], []
+    ys = np.ascontiguousarray(wl.youngs_scale[pick], np.float32)
+    fs = np.ascontiguousarray(wl.friction_scale[pick], np.float32)
+    for r, i in enumerate(pick):
+        o = oracle64.straight(64, 1.0, youngs=1e8, poisson=0.3, density=1100.0, radius=5e-3, direction=(0, 0, -1))
+        oracle64.pin(o, 0)
+        orods.append(o)
+        protos.append(product_rod(o))
+        oworlds.append(OW([OP.plane((0, 0, -1.2), (0, 0, 1), 0.5 * float(fs[r]))]))
+        worlds.append(rp.World([rp.Primitive.plane((0, 0, -1.2), (0, 0, 1), 0.5)]))
+    drives = [wl.drives[i] for i in pick]
+
+    def kin(s):
+        t = s * p.dt
+        return np.array([[0.0, 0.0, d.amplitude * 2 * math.pi * d.frequency *
+                          math.cos(2 * math.pi * d.frequency * t + d.phase)] for d in drives])
+
+    # the reference batch takes the friction scale as a material scale, the
+    # FP64 worlds carry it in the floor's coefficient
+    ref_worlds = [OW([OP.plane((0, 0, -1.2), (0, 0, 1), 0.5)]) for _ in pick]
+    rows = _run_three(R, orods, oworlds, oparams(p), protos, worlds, p, (1, 10, 100, 1000), kin, (ys, fs),
+                      ref_worlds)
+    _print_rows("grid", rows)
+    assert rows[1]["reference order"] <= 1e-5 and rows[1]["mixed"] <= 1e-6
+    assert rows[1000]["mixed"] <= rows[1000]["reference order"] + 1e-7
+
+
+def test_error_vs_fp64_uneven(reference_gpu, oracle64):
+    """Config 3, 8 rods sampled from the uneven batch, 50 steps."""
+    R = reference_gpu
+    _need(R)
+    draws = synth.uneven(16384, 0)
+    idx = np.random.default_rng(11).choice(len(draws), size=8, replace=False)
+    p = rp.StepParams(dt=1.0 / 60, substeps=50, iterations=1)
+    orods, oworlds, protos, worlds = [], [], [], []
+    for i in idx:
+        d = draws[i]
+        o = oracle64.centerline(d.points, youngs=synth.YOUNGS, poisson=synth.POISSON, density=synth.DENSITY,
+                                radius=synth.RADIUS, frame_seed=(0, 0, 1))
+        o.bRestD[:] = 0.0
+        orods.append(o)
+        protos.append(product_rod(o))
+        oworlds.append(OW([OP(*q) for q in d.prims], True, d.friction, 2, d.hash_table_size, 0.25))
+        worlds.append(rp.World([W.primitive(q) for q in d.prims], self_collision=True, self_friction=d.friction,
+                               hash_table_size=d.hash_table_size))
+    rows = _run_three(R, orods, oworlds, oparams(p), protos, worlds, p, (1, 10, 50))
+    _print_rows("uneven", rows)
+    assert rows[1]["reference order"] <= 1e-5 and rows[1]["mixed"] <= 1e-6
+
+
+def test_error_vs_fp64_hook(reference_gpu, oracle64):
+    """Config 4, 8 placements over the sweep, the full 480 steps (8 s)."""
+    R = reference_gpu
+    _need(R)
+    p = rp.StepParams(dt=1.0 / 60, substeps=20, iterations=1)
+    orods, oworlds, protos, worlds = [], [], [], []
+    for k in range(8):
+        ratio, mu, youngs = 1.0 + 3.0 * k / 7, 0.05 + 0.55 * ((3 * k) % 8) / 7, (1e8, 3e8)[k % 2]
+        o = oracle64.centerline(W.hanging_cable_points(ratio), youngs=youngs, frame_seed=(0, 1, 0),
+                                **W.HOOK_MATERIAL)
+        o.bRestD[:] = 0.0
+        orods.append(o)
+        protos.append(product_rod(o))
+        oworlds.append(OW([OP.capsule((0.0, -0.3, 0.8), (0.0, 0.3, 0.8), 0.02, mu),
+                           OP.plane((0, 0, 0), (0, 0, 1), mu)], True, mu, 2, 256, 0.25))
+        worlds.append(rp.World([rp.Primitive.capsule((0.0, -0.3, 0.8), (0.0, 0.3, 0.8), 0.02, mu),
+                                rp.Primitive.plane((0, 0, 0), (0, 0, 1), mu)],
+                               self_collision=True, self_friction=mu, hash_table_size=256))
+    rows = _run_three(R, orods, oworlds, oparams(p), protos, worlds, p, (1, 10, 100, 480))
+    _print_rows("hook", rows)
+    assert rows[1]["reference order"] <= 1e-5 and rows[1]["mixed"] <= 1e-6

@@ -10,11 +10,13 @@ steps (50 ms) and at the end; held <=> max rise <= 0.05 m.
 
 The 200 placements nearest the capstan boundary mu = ln(ratio) / pi are
 re-run on the reference's own FP64 CPU solver (compiled from its sources,
-colour-ordered, observed by its own HangOutcome) and on its own FP32 GPU
-batch (run as its harness runs a sweep). These are the placements where
-single precision is known to flip verdicts; the mixed-precision mode's
-agreement with FP64 is asserted (>= 180 of 200, and no less than the
-reference GPU kernel's), and printed for the reference-order FP32 mode too.
+colour-ordered, observed by its own HangOutcome) and, the way the
+reference's harness runs a sweep, on its own FP32 GPU batch and on this
+library in the reference's FP32 order. These are the placements where single
+precision is known to flip verdicts. Asserted: this library's reference-order
+verdicts equal the reference kernel's bit for bit; the mixed-precision
+mode's agreement with FP64 is at least its measured count and no less than
+the reference kernel's.
 """
 import math
 import os
@@ -43,14 +45,18 @@ def gpu_verdicts(wl, precision):
     return rise, held, near
 
 
-def reference_gpu_verdicts(ratios, mus, youngs, p):
-    """Hold/slide of the given placements on the reference's own GPU batch,
-    run the way its harness runs a sweep (heldOnGpu,
-    src/validation/application_cases.cpp:38-70): one fused batch per
-    (friction, stiffness) -- the batch shares one world and one prototype --
-    every ratio uploaded as a rod, HangOutcome from the rod's double start
-    height and the downloaded FP32 positions every INTERVAL steps and at the
-    end. None without the reference GPU build."""
+def harness_style_verdicts(ratios, mus, youngs, p):
+    """Hold/slide of the given placements on the reference's own GPU batch and
+    on this library, both run the way the reference's harness runs a sweep
+    (heldOnGpu, src/validation/application_cases.cpp:38-70): one batch per
+    (friction, stiffness), created from the group's first cable -- the batch
+    shares that prototype's rest data and one world -- with every cable's
+    state uploaded as a rod (Batch::uploadRod), HangOutcome from the cable's
+    double start height and the FP32 positions every INTERVAL steps and at
+    the end. This library runs in the reference's FP32 order, observed on the
+    device. Returns (held_reference, rise_reference, held_ours, rise_ours,
+    rods whose final positions are bitwise equal), or None without the
+    reference GPU build."""
     try:
         from oracle import Reference
         R = Reference(gpu=True)
@@ -59,24 +65,38 @@ def reference_gpu_verdicts(ratios, mus, youngs, p):
     if not R.lib.refgpu_available():
         return None
     import ctypes as C
-    held = np.zeros(len(ratios), np.uint8)
+    from tests.helpers import product_rod
+    n_all = len(ratios)
+    held_g, rise_g = np.zeros(n_all, np.uint8), np.zeros(n_all)
+    held_o, rise_o = np.zeros(n_all, np.uint8), np.zeros(n_all)
+    same = 0
     g = (C.c_double * 3)(*p.gravity)
     fp = C.POINTER(C.c_float)
+    params = rp.StepParams(dt=1.0 / 60, substeps=20, iterations=1)
     groups = {}
     for n, key in enumerate(zip(mus, youngs)):
         groups.setdefault(key, []).append(n)
     for (mu, E), members in groups.items():
         handles = [R.hanging(float(ratios[n]), float(E), length=1.2, segments=120, bar_radius=0.02,
                              bar_height=0.8) for n in members]
-        wh = R.world(OW([OP.capsule((0, -0.3, 0.8), (0, 0.3, 0.8), 0.02, float(mu)),
-                         OP.plane((0, 0, 0), (0, 0, 1), float(mu))],
-                        self_collision=True, self_friction=float(mu), hash_table_size=256))
-        rb = R.lib.refgpu_create(handles[0], len(members), 1, wh)
+        ow = OW([OP.capsule((0, -0.3, 0.8), (0, 0.3, 0.8), 0.02, float(mu)),
+                 OP.plane((0, 0, 0), (0, 0, 1), float(mu))],
+                self_collision=True, self_friction=float(mu), hash_table_size=256)
+        rb = R.lib.refgpu_create(handles[0], len(members), 1, R.world(ow))
         assert rb
+        cables = [product_rod(R.export(h)) for h in handles]
+        world = rp.World([rp.Primitive.capsule((0, -0.3, 0.8), (0, 0.3, 0.8), 0.02, float(mu)),
+                          rp.Primitive.plane((0, 0, 0), (0, 0, 1), float(mu))],
+                         self_collision=True, self_friction=float(mu), hash_table_size=256)
+        b = rp.Batch.create(cables[0], len(members), rp.Strategy.BATCHED, world)
         z0 = []
         for r, h in enumerate(handles):
             R.lib.refgpu_upload_rod(rb, r, h)
-            z0.append(float(R.export(h).x[0][2]))
+            b.upload_rod(r, cables[r])
+            z0.append(float(cables[r].x[0][2]))
+        b.arm_hold_observer([0] * len(members), interval=INTERVAL, tolerance=0.05, start_z=z0)
+        b.set_graph(True)
+        b.step_many(params, STEPS)
         pos = np.zeros((len(members), 121, 3), np.float32)
         rise = np.zeros(len(members))
         for s in range(1, STEPS + 1):
@@ -84,12 +104,17 @@ def reference_gpu_verdicts(ratios, mus, youngs, p):
             if s % INTERVAL == 0 or s == STEPS:
                 R.lib.refgpu_download_positions(rb, pos.ctypes.data_as(fp))
                 rise = np.maximum(rise, pos[:, 0, 2].astype(np.float64) - np.array(z0))
+        mine = b.download_positions().reshape(len(members), 121, 3)
+        same += int(np.sum(np.all(mine == pos, axis=(1, 2))))
+        r_o, h_o, _ = b.read_hold_verdicts()
         for r, n in enumerate(members):
-            held[n] = 1 if rise[r] <= 0.05 else 0
+            held_g[n], rise_g[n] = (1 if rise[r] <= 0.05 else 0), rise[r]
+            held_o[n], rise_o[n] = h_o[r], r_o[r]
+        b.close()
         R.lib.refgpu_free(rb)
         for h in handles:
             R.free(h)
-    return held
+    return held_g, rise_g, held_o, rise_o, same
 
 
 def test_hook_sweep_verdicts_vs_fp64_cpu(reference):
@@ -123,15 +148,28 @@ def test_hook_sweep_verdicts_vs_fp64_cpu(reference):
     rise_c, held_c = reference.hold_many(handles, worlds, p, STEPS, INTERVAL, os.cpu_count() or 1)
     for h in handles:
         reference.free(h)
-    held_g = reference_gpu_verdicts(ratios[r_i[nearest]], mus[m_i[nearest]], [Es[e] for e in e_i[nearest]], p)
+    harness = harness_style_verdicts(ratios[r_i[nearest]], mus[m_i[nearest]], [Es[e] for e in e_i[nearest]], p)
     agree_m = int(np.sum(held_m[nearest] == held_c))
     agree_f = int(np.sum(held_f[nearest] == held_c))
-    agree_g = int(np.sum(held_g == held_c)) if held_g is not None else None
+    margin = np.abs(rise_c - 0.05)
+    flips = np.nonzero(held_m[nearest] != held_c)[0]
     print(f"\nhook sweep: held {held_m.sum()}/3600 (mixed) {held_f.sum()}/3600 (FP32); "
           f"200 nearest the capstan boundary: mixed agrees {agree_m}/200, FP32 {agree_f}/200, "
-          f"reference GPU kernel (FP32) {agree_g}/200, near-boundary flags {int(near_m[nearest].sum())}")
-    assert agree_m >= 180
-    if agree_g is not None:  # the mixed mode agrees with FP64 at least as often as the reference kernel
+          f"near-boundary flags {int(near_m[nearest].sum())}; FP64 rise margins |rise - 0.05| of the "
+          f"mixed-mode disagreements: {sorted(np.round(margin[flips], 4).tolist())}")
+    if harness is not None:
+        held_g, rise_g, held_o, rise_o, same = harness
+        agree_g = int(np.sum(held_g == held_c))
+        print(f"harness-style runs of the 200: reference GPU kernel agrees with FP64 on {agree_g}/200; "
+              f"this library in its FP32 order equals the reference kernel's verdicts on "
+              f"{int(np.sum(held_o == held_g))}/200, max |rise - rise_ref| {np.max(np.abs(rise_o - rise_g)):.2e} m, "
+              f"final positions bitwise equal on {same}/200")
+        # reference-order verdicts are the reference kernel's, bit for bit
+        assert np.array_equal(held_o, held_g)
+        # the mixed mode agrees with FP64 at least as often as the reference kernel
         assert agree_m >= agree_g
+    # measured: 184 of 200 (the disagreements are listed above with their
+    # FP64 margins); a regression below that fails
+    assert agree_m >= 184
     # the sweep is not degenerate: both outcomes occur
     assert 0 < held_m.sum() < 3600

@@ -13,9 +13,10 @@ gpu::Batch and run end to end (src/gpu/gpu_suite.cpp:836-954).
   suite's checks.
 * With compensated positions and the FP64 friction cone
   (RP_B200_PRECISION=3) the incline at 8 substeps, which the reference marks
-  as beyond float ("slip angle 13.5 %"), lands inside its 5 % slip-angle
-  tolerance, and the capstan agrees with the colour-ordered FP64 CPU solver
-  within the suite's agreement bound (0.01).
+  as beyond float ("slip angle 13.5 %"), lands inside its bounds (slip angle
+  5 %, effective mu while sliding 8 %): the contact constraint is measured on
+  the compensated positions. The capstan agrees with the colour-ordered FP64
+  CPU solver within the suite's agreement bound (0.01).
 """
 import os
 import re
@@ -72,8 +73,9 @@ def test_mixed_precision_incline_within_tolerance():
     print(f"\nincline at 8 substeps: FP32 slip {fp32[slip][0]} mu {fp32[mu][0]}; "
           f"mixed slip {mixed[slip][0]} mu {mixed[mu][0]}")
     assert float(fp32[slip][0]) > 0.05  # the float limit the reference reports
-    assert float(mixed[slip][0]) < 0.05  # its tolerance (src/gpu/gpu_suite.cpp)
-    assert float(mixed[mu][0]) < float(fp32[mu][0]) / 3
+    # the reference's own bounds for the incline (src/gpu/gpu_suite.cpp:640-645)
+    assert float(mixed[slip][0]) <= 0.05
+    assert float(mixed[mu][0]) <= 0.08
 
 
 def test_mixed_precision_capstan_agrees_with_fp64_cpu():

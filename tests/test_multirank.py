@@ -1,11 +1,12 @@
 """The multi-rank host logic of bench.py on CPU (gloo, world size 2).
 
-Rods are independent, so N ranks each simulate their own seeded shard of the
-workload with no data-path collective; the only cross-rank steps are the
-barrier around the timed region and the max-over-ranks of the step time.
-This runs those steps as two gloo ranks and checks that the shards differ,
-that both ranks see the max of the two times, and that the reference arm
-prints nothing on rank 1.
+Rods are independent, so N ranks each simulate their own shard of one seeded
+batch of N x rods (sorted by length, every N-th rod) with no data-path
+collective; the only cross-rank steps are the barrier around the timed region
+and the max-over-ranks of the step time. This runs those steps as two gloo
+ranks and checks that the shards are disjoint, cover the batch and are
+balanced, that both ranks see the max of the two times, and that the
+reference arm prints nothing on rank 1.
 """
 import io
 import os
@@ -38,7 +39,7 @@ def _rank(rank, world, port, out):
 
     w, r, _ = bench.dist_setup(A)
     assert (w, r) == (world, rank) and dist.get_backend() == "gloo"
-    wl = bench.build_workload("uneven", 6, seed=A.seed + r)
+    wl = bench.build_workload("uneven", 6, seed=A.seed, shard=(r, w))
     bench.barrier(w)
     t = bench.max_over_ranks(1.5 + r, w)
     shards = [None] * w
@@ -69,8 +70,14 @@ def test_two_gloo_ranks():
             assert p.exitcode == 0
         res = dict(out)
     assert set(res) == {0, 1}
+    from ropephysics_b200 import synth
+    whole = sorted(d.segments for d in synth.uneven(12, 5))
     for r in (0, 1):
         t, shards, printed = res[r]
         assert t == 2.5
-        assert shards[0] != shards[1]  # each rank its own seeded shard
+        # the two shards of one seeded batch: disjoint, together the batch,
+        # each the same spread of lengths (every other rod by length)
+        assert sorted(shards[0] + shards[1]) == whole
+        assert len(shards[0]) == len(shards[1]) == 6
+        assert abs(sum(shards[0]) - sum(shards[1])) <= max(whole)
     assert res[1][2] == ""  # the reference arm runs on rank 0 alone
