@@ -328,14 +328,18 @@ rp_status rp_batch_step_many(rp_batch* batch, const rp_step_params* params, int3
 /* No reference counterpart. One step of an RP_STRATEGY_BATCHED batch, the
  * same kernel and the same results as rp_batch_step, but the step's scratch
  * (work-queue counters, start-of-substep frames under compensated
- * precision, world-contact slots, self-contact pool) is carved from a fixed static device array of
+ * precision, world-contact slots, self-contact pool, hash, sort and
+ * projection levels, constraint multipliers) is carved from a fixed static
+ * device array of
  * RP_STATIC_SCRATCH_BYTES instead of the batch's own buffers, and the call
  * allocates no device memory. Needs 256 bytes, plus 16 x frames under
  * RP_PRECISION_COMPENSATED, plus 32 x contact slots when the batch's plan
  * keeps the slots in global memory (rods with many or large contact
- * primitives), plus 64 x self-contact pool entries when any rod collides with
- * itself, each section rounded up to 256 bytes; a larger batch is rejected
- * with RP_ERR_INVALID. The batch's device must be
+ * primitives), plus, when any rod collides with itself, 64 x self-contact
+ * pool entries, 4 x (2 (hash_table_size + 1) + 3 (pool capacity + 1)) per
+ * such rod and 8 x stretch constraints, plus 16 x (stretch + bend
+ * constraints) when params->iterations > 1, each section rounded up to 256
+ * bytes; a larger batch is rejected with RP_ERR_INVALID. The batch's device must be
  * current. The first call on a device looks up the array's address, once;
  * make that first call before any stream capture. The queue counters are
  * cleared on the batch's stream before each launch; nothing else needs to

@@ -197,7 +197,10 @@ static rp_status createImpl(const rp_rod_desc* const* rods, int numRods, const r
         b->totalB += T.nB;
         b->totalSlots += int64_t(T.nP) * R.numPrims;
         b->totalPool += R.selfCapacity;
-        b->totalHash += R.selfCollision ? R.hashTableSize + 1 : 0;
+        if (R.selfCollision)
+            b->totalHash += strategy == RP_STRATEGY_BATCHED
+                                ? 2 * int64_t(R.hashTableSize + 1) + 3 * int64_t(R.selfCapacity + 1)
+                                : int64_t(R.hashTableSize) + 1;
         b->maxPrims = std::max(b->maxPrims, R.numPrims);
         b->anySelf = b->anySelf || R.selfCollision;
         const rp::RodLayout L = rp::rodLayout(T.nP, T.nS, T.nSt, T.nB, R.numPrims, R.selfCollision,
@@ -207,7 +210,8 @@ static rp_status createImpl(const rp_rod_desc* const* rods, int numRods, const r
         b->tmplNP[r] = T.nP;
         b->tmplNS[r] = T.nS;
     }
-    if (b->totalP > (int64_t(1) << 31) - 1 || b->totalS > (int64_t(1) << 31) - 1)
+    if (b->totalP > (int64_t(1) << 31) - 1 || b->totalS > (int64_t(1) << 31) - 1 ||
+        b->totalHash > (int64_t(1) << 31) - 1)
         return guard(fail(RP_ERR_INVALID, "batch exceeds 2^31 particles"));
 
     const size_t optin = optinSmem(b->device);
@@ -298,6 +302,12 @@ static rp_status createImpl(const rp_rod_desc* const* rods, int numRods, const r
     } else if (strategy == RP_STRATEGY_BATCHED) {
         // the lean shared-memory layout keeps these in global memory
         ALLOC(A.gqPrev, float4, S);
+        ALLOC(A.gLamS, float4, size_t(b->totalSt));  // read only at more than one iteration
+        ALLOC(A.gLamB, float4, size_t(b->totalB));
+        if (b->anySelf) {
+            ALLOC(A.gSelfInt, int32_t, 2 * size_t(b->totalSt));
+            ALLOC(A.gHash, int32_t, size_t(b->totalHash));
+        }
         ALLOC(A.gSlots, rp::DSlot, size_t(b->totalSlots));
         if (b->anySelf) ALLOC(A.gPool, rp::DSelf, size_t(b->totalPool));
     }
@@ -644,14 +654,20 @@ rp_status rp_batch_step_static_scratch(rp_batch* b, const rp_step_params* p) {
     // from global memory: work-queue counters; start-of-substep frames
     // (compensated precision: otherwise they live in shared memory);
     // world-contact slots (unless the plan keeps them in shared memory);
-    // self-contact pool (when a rod collides with itself)
+    // self-contact pool, hash, sort and levels (when a rod collides with
+    // itself); constraint multipliers (more than one iteration)
     auto up = [](size_t n) { return (n + 255) & ~size_t(255); };
     const bool comp = (b->precision & RP_PRECISION_COMPENSATED) != 0;
     const bool globalSlots = b->a.slotsShared == 0 && b->totalSlots > 0;
     const size_t qPrevAt = 256;
     const size_t slotsAt = qPrevAt + (comp ? up(size_t(b->totalS) * sizeof(float4)) : 0);
     const size_t poolAt = slotsAt + (globalSlots ? up(size_t(b->totalSlots) * sizeof(rp::DSlot)) : 0);
-    const size_t need = poolAt + (b->anySelf ? up(size_t(b->totalPool) * sizeof(rp::DSelf)) : 0);
+    const bool lambdas = p->iterations > 1;  // one iteration needs no multipliers
+    const size_t hashAt = poolAt + (b->anySelf ? up(size_t(b->totalPool) * sizeof(rp::DSelf)) : 0);
+    const size_t sortAt = hashAt + (b->anySelf ? up(size_t(b->totalHash) * sizeof(int32_t)) : 0);
+    const size_t lamSAt = sortAt + (b->anySelf ? up(2 * size_t(b->totalSt) * sizeof(int32_t)) : 0);
+    const size_t lamBAt = lamSAt + (lambdas ? up(size_t(b->totalSt) * sizeof(float4)) : 0);
+    const size_t need = lamBAt + (lambdas ? up(size_t(b->totalB) * sizeof(float4)) : 0);
     void* base = nullptr;
     size_t have = 0;
     const cudaError_t e = rp::staticScratch(&base, &have);
@@ -667,6 +683,10 @@ rp_status rp_batch_step_static_scratch(rp_batch* b, const rp_step_params* p) {
     A.gqPrev = comp ? reinterpret_cast<float4*>(s + qPrevAt) : nullptr;
     A.gSlots = globalSlots ? reinterpret_cast<rp::DSlot*>(s + slotsAt) : nullptr;
     A.gPool = b->anySelf ? reinterpret_cast<rp::DSelf*>(s + poolAt) : nullptr;
+    A.gHash = b->anySelf ? reinterpret_cast<int32_t*>(s + hashAt) : nullptr;
+    A.gSelfInt = b->anySelf ? reinterpret_cast<int32_t*>(s + sortAt) : nullptr;
+    A.gLamS = lambdas ? reinterpret_cast<float4*>(s + lamSAt) : nullptr;
+    A.gLamB = lambdas ? reinterpret_cast<float4*>(s + lamBAt) : nullptr;
     rp::BatchedPlan plan;
     plan.groups = b->dGroups;
     plan.numGroups = b->numGroups;

@@ -361,17 +361,19 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
     V.kin = A.kinVel + R.pOff;
     V.omega = reinterpret_cast<float4*>(base + L.omega);
     V.torque = A.torque + R.sOff;
-    V.lamS = reinterpret_cast<float4*>(base + L.lamS);
-    V.lamB = reinterpret_cast<float4*>(base + L.lamB);
+    // multipliers: none at one iteration; else in global memory (L1/L2)
+    V.lamS = A.iterations > 1 ? A.gLamS + R.stOff : nullptr;
+    V.lamB = A.iterations > 1 ? A.gLamB + R.bOff : nullptr;
     V.slots = A.slotsShared ? reinterpret_cast<DSlot*>(base + L.slots) : A.gSlots + R.slotOff;
     SelfScratch Sb;
 #define S Sb
     S.centres = reinterpret_cast<float4*>(base + L.centres);
-    S.cellOf = reinterpret_cast<int32_t*>(base + L.selfInt);
-    S.sorted = S.cellOf + nSt;
-    S.segCount = S.sorted + nSt;
+    S.segCount = reinterpret_cast<int32_t*>(base + L.selfInt);
     S.segStart = S.segCount + nSt;
-    S.cellStart = reinterpret_cast<int32_t*>(base + L.hash);
+    // touched only on substeps where a pair touches: global memory (L1/L2)
+    S.cellOf = A.gSelfInt + 2 * int64_t(R.stOff);
+    S.sorted = S.cellOf + nSt;
+    S.cellStart = A.gHash + R.hashOff;  // then the cursors, then the levels
     S.pool = A.gPool + R.poolOff;
     int32_t* misc = reinterpret_cast<int32_t*>(base + L.misc);
     S.cellSize = reinterpret_cast<float*>(misc);
@@ -390,7 +392,7 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
         C.primMask = reinterpret_cast<unsigned long long*>(misc + 12);
         C.touching = misc + 14;
         C.red = reinterpret_cast<float*>(misc + 16);  // 8 floats per warp
-        C.lvlOrder = reinterpret_cast<int32_t*>(base + L.levels);
+        C.lvlOrder = C.cursor + (R.hashTableSize + 1);
         C.lvlStart = C.lvlOrder + (R.selfCapacity + 1);
         C.lvlOf = C.lvlStart + (R.selfCapacity + 1);
         C.sOrder = A.tOrder + T.sOrderOff;
@@ -470,8 +472,10 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
         }
         teamSync(team, teamIdx);
         for (int sub = 0; sub < A.substeps; ++sub) {
-            for (int k = lane; k < nSt; k += team) V.lamS[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            for (int k = lane; k < nB; k += team) V.lamB[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (V.lamS) {  // team-uniform
+                for (int k = lane; k < nSt; k += team) V.lamS[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                for (int k = lane; k < nB; k += team) V.lamB[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            }
             const bool regenerate = sub % interval == 0;
             unsigned long long maskNow = *primMask;  // this substep's primitive cull
             float cellNow = 0.0f;                    // this substep's self-collision cell

@@ -43,12 +43,16 @@ struct DTemplate {
 struct DRod {
     int32_t tmpl;
     int32_t pOff, sOff;            // particle / frame state offsets (16-byte aligned rows)
-    int32_t stOff, bOff;           // multiplier scratch offsets (global-memory strategy)
+    int32_t stOff, bOff;           // per-rod stretch / bend scratch offsets (multipliers,
+                                   // sort arrays) in global memory
     int32_t primOff, numPrims;     // slice of the primitive array
     int64_t slotOff;               // contact slot offset: pOff * maxPrims
     int32_t selfCollision, selfGap, selfCapacity, hashTableSize;
     int32_t poolOff;               // self-contact pool offset (selfCapacity entries)
-    int32_t hashOff;               // hash-table scratch offset (hashTableSize + 1 ints)
+    int32_t hashOff;               // self-contact scratch offset into gHash: the plain
+                                   // kernel's hash (hashTableSize + 1 ints); the batched
+                                   // kernel's hash, cursors and levels
+                                   // (2 (hashTableSize + 1) + 3 (selfCapacity + 1) ints)
     float contactMargin;           // world.contactMarginRadii * radius
     float selfFriction;
     float radius;
@@ -150,15 +154,17 @@ struct DArgs {
     float4* xComp;  // Kahan compensation of x (RP_PRECISION_COMPENSATED)
     float4* qComp;          // per frame: Kahan compensation of q (compensated precision)
 
-    // scratch used in place of shared memory by the global-memory strategy
+    // scratch in global memory: the global-memory strategy's whole state, and
+    // what the batched kernel keeps off chip
     float4* gxPrev;
     float4* gqPrev;
     float4* gLamS;
     float4* gLamB;
     DSlot* gSlots;
     float4* gCentres;  // per segment
-    int32_t* gSelfInt; // 4 ints per segment: cellOf, sorted, count, start
-    int32_t* gHash;    // hashTableSize + 1 per rod
+    int32_t* gSelfInt; // per segment: plain kernel 4 ints (cellOf, sorted, count,
+                       // start) at 4 stOff; batched 2 ints (cellOf, sorted) at 2 stOff
+    int32_t* gHash;    // per rod at hashOff (see DRod::hashOff)
     DSelf* gPool;      // selfCapacity per rod
     int32_t* gMisc;    // 4 per rod: cell size (float bits), live, overflow, pad
 

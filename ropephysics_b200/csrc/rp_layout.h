@@ -6,24 +6,29 @@
 // lean layout (batched kernel) keeps what every substep reads and writes --
 // positions and their start-of-substep copies, frames and (except under
 // compensation, where the shared memory is worth more as occupancy) their
-// start-of-substep copies, velocities, angular velocities, multipliers, the
-// hash -- and leaves in global memory what a step only reads (loads,
+// start-of-substep copies, velocities, angular velocities, the self-contact
+// count's centres -- and leaves in global memory what a step only reads (loads,
 // kinematic velocities) or touches only when a contact is live (world
 // contact slots of primitives that survive the per-rod cull, the
-// self-contact pool); those stay L1/L2-resident. `slotsShared` moves the
+// self-contact hash, sort, pool and projection levels); those stay
+// L1/L2-resident. `slotsShared` moves the
 // world contact slots into the lean layout too, for batches whose groups
 // still fit as many CTAs per SM with them.
 //   frames     q, qPrev (not lean+comp), omega [, torque]  16 x nS each
 //   particles  x, xPrev, v [, force, kin], xComp     16 x nP each (xComp: full,
 //                                                    or lean with compensation)
 //   frames     qComp                                 16 x nS (lean with compensation)
-//   lambdas    stretch, bend                         16 x (nSt + nB)
+//   lambdas    stretch, bend                         16 x (nSt + nB) (full only: the
+//                                                    batched kernel needs none at
+//                                                    one iteration, else keeps
+//                                                    them in global memory)
 //   slots      [world contacts]                      32 x nP x numPrims (full, or lean
 //                                                    with slotsShared)
 //   misc       kMiscBytes (below)
-//   self       centres 16 nSt, ints 16 nSt, hash + cursor 2 x 4 (table + 1),
-//              [pool 64 x capacity], projection levels 3 x 4 (capacity + 1),
-//              [chain-block bounds 32 x ceil(nSt / 8)] (lean)
+//   self       full: centres 16 nSt, ints 16 nSt, hash 4 (table + 1) x 2,
+//              pool 64 x capacity, projection levels 3 x 4 (capacity + 1);
+//              lean: centres 16 nSt, count and start 8 nSt, chain-block
+//              bounds 32 x ceil(nSt / 8) (the rest in global memory)
 #pragma once
 
 #include <cstdint>
@@ -86,29 +91,33 @@ RP_HD inline RodLayout rodLayout(int32_t nP, int32_t nS, int32_t nSt, int32_t nB
     } else {
         L.qComp = -1;  // the plain kernel keeps it in global memory
     }
-    L.lamS = o;   o += 16 * nSt;
-    L.lamB = o;   o += 16 * nB;
+    if (!lean) {  // lean: none at one iteration, else in global memory
+        L.lamS = o;   o += 16 * nSt;
+        L.lamB = o;   o += 16 * nB;
+    } else {
+        L.lamS = L.lamB = -1;
+    }
     if (!lean || slotsShared) {
         L.slots = o;  o += 32 * nP * nPrims;
     } else {
         L.slots = -1;
     }
     L.misc = o;        o += kMiscBytes;
-    if (self) {
+    if (self && !lean) {
         L.centres = o; o += 16 * nSt;
         L.selfInt = o; o += 16 * nSt;
         L.hash = o;    o += rpAlign16(8 * (table + 1));
-        if (!lean) {
-            L.pool = o;    o += 64 * capacity;
-        } else {
-            L.pool = -1;
-        }
+        L.pool = o;    o += 64 * capacity;
         L.levels = o;  o += rpAlign16(12 * (capacity + 1));
-        if (lean) {
-            L.blocks = o;  o += 32 * ((nSt + 7) / 8);
-        } else {
-            L.blocks = -1;
-        }
+        L.blocks = -1;
+    } else if (self) {
+        // lean: what the count reads every substep; the hash, the sort and
+        // the projection levels (touched only while a pair touches) and the
+        // pool live in global memory
+        L.centres = o; o += 16 * nSt;
+        L.selfInt = o; o += 8 * nSt;  // per-segment count and start
+        L.hash = L.pool = L.levels = -1;
+        L.blocks = o;  o += 32 * ((nSt + 7) / 8);
     } else {
         L.centres = L.selfInt = L.hash = L.pool = L.levels = o;
         L.blocks = -1;

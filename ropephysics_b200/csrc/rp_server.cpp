@@ -91,7 +91,7 @@ class RangeAlloc {
     int64_t cap_ = 0;
 };
 
-enum Unit { TP, TS, TST, TB, ORD, CS, TMPL, ROD, SP, SS, SLOT, POOL, PRIM, NUNITS };
+enum Unit { TP, TS, TST, TB, ORD, CS, TMPL, ROD, SP, SS, SLOT, POOL, PRIM, HASH, NUNITS };
 
 // Device bytes per element of each unit (all arrays of that unit).
 constexpr int64_t kUnitBytes[NUNITS] = {
@@ -106,10 +106,13 @@ constexpr int64_t kUnitBytes[NUNITS] = {
     // order, group row
     int64_t(sizeof(rp::DRod)) + 8 + int64_t(sizeof(rp::DDrive)) + 8 + 4 + 8 + 4 + 16,
     5 * 16,                                      // SP   x, v, force, kin, xComp
-    5 * 16,                                      // SS   q, omega, torque, qPrev, qComp
+    7 * 16 + 8,                                  // SS   q, omega, torque, qPrev, qComp, and by
+                                                 //      frame range the multipliers and the
+                                                 //      self-contact sort (2 ints)
     int64_t(sizeof(rp::DSlot)) + 1,              // SLOT slots + contact state
     int64_t(sizeof(rp::DSelf)) + 4,              // POOL pool + pair list
     int64_t(sizeof(rp::DPrim)),                  // PRIM
+    4,                                           // HASH self-contact hash, cursors, levels
 };
 
 // Whole steps per server launch (fewer host round trips; admission happens
@@ -246,9 +249,12 @@ bool rp_server::admit(Request& rq) {
         R.tmpl += int32_t(o[TMPL]);
         R.pOff += int32_t(o[SP]);
         R.sOff += int32_t(o[SS]);
+        R.stOff = R.sOff;  // multipliers and sort arrays by the rod's frame range
+        R.bOff = R.sOff;
         R.primOff += int32_t(o[PRIM]);
         R.slotOff += o[SLOT];
         R.poolOff += int32_t(o[POOL]);
+        R.hashOff += int32_t(o[HASH]);
         rq.rodIds[i] = int32_t(o[ROD]) + i;
         hRods[size_t(o[ROD]) + i] = R;
     }
@@ -488,6 +494,7 @@ rp_status rp_server_create(const rp_server_config* cfg, rp_server** out) {
         cap[SLOT] = 2 * P;
         cap[POOL] = P / 2 + 16 * cap[ROD];
         cap[PRIM] = 8 * cap[ROD];
+        cap[HASH] = 12 * P;  // tables of 2..4 buckets per segment, levels of half as many
         int64_t bytes = 0;
         for (int u = 0; u < NUNITS; ++u) bytes += cap[u] * kUnitBytes[u];
         return bytes;
@@ -532,6 +539,10 @@ rp_status rp_server_create(const rp_server_config* cfg, rp_server** out) {
          s->dalloc(A.kinVel, cap[SP]) && s->dalloc(A.xComp, cap[SP]);
     ok = ok && s->dalloc(A.q, cap[SS]) && s->dalloc(A.omega, cap[SS]) && s->dalloc(A.torque, cap[SS]) &&
          s->dalloc(A.gqPrev, cap[SS]) && s->dalloc(A.qComp, cap[SS]);
+    // multipliers (read only at more than one iteration) and the self-contact
+    // sort live in a rod's frame range (its constraint counts are <= its frames)
+    ok = ok && s->dalloc(A.gLamS, cap[SS]) && s->dalloc(A.gLamB, cap[SS]);
+    ok = ok && s->dalloc(A.gSelfInt, 2 * cap[SS]) && s->dalloc(A.gHash, cap[HASH]);
     ok = ok && s->dalloc(A.gSlots, cap[SLOT]) && s->dalloc(A.contactState, cap[SLOT]);
     ok = ok && s->dalloc(A.gPool, cap[POOL]) && s->dalloc(A.selfPairs, cap[POOL]);
     ok = ok && s->dalloc(A.selfCount, cap[ROD]) && s->dalloc(A.selfOverflow, cap[ROD]) &&
@@ -602,6 +613,10 @@ rp_status rp_server_submit(rp_server* s, const rp_request* r, uint64_t* id) {
         if (it == tmplOf.end()) {
             const std::string why = rpx::validateDesc(d);
             if (!why.empty()) return fail(RP_ERR_INVALID, "rod " + std::to_string(i) + ": " + why);
+            if (d->num_stretch > d->num_frames || d->num_bend > d->num_frames)
+                return fail(RP_ERR_INVALID, "rod " + std::to_string(i) +
+                                                ": the server needs at most as many stretch and bend "
+                                                "constraints as frames (every chain has)");
             rpx::TemplateHost th;
             rpx::makeTemplate(d, th);
             rp::DTemplate T = th.T;
@@ -656,6 +671,7 @@ rp_status rp_server_submit(rp_server* s, const rp_request* r, uint64_t* id) {
         }
         R.slotOff = Q.counts[SLOT];
         R.poolOff = int32_t(Q.counts[POOL]);
+        R.hashOff = int32_t(Q.counts[HASH]);
         Q.rods.push_back(R);
         const size_t p0 = Q.x.size(), s0 = Q.q.size();
         Q.x.resize(p0 + T.nP);
@@ -692,6 +708,8 @@ rp_status rp_server_submit(rp_server* s, const rp_request* r, uint64_t* id) {
         Q.rodNP.push_back(T.nP);
         Q.counts[SLOT] += int64_t(T.nP) * R.numPrims;
         Q.counts[POOL] += R.selfCapacity;
+        if (R.selfCollision)
+            Q.counts[HASH] += 2 * int64_t(R.hashTableSize + 1) + 3 * int64_t(R.selfCapacity + 1);
         Q.particles += T.nP;
         Q.segmentSubsteps += int64_t(T.nSt) * substeps * r->steps;
     }

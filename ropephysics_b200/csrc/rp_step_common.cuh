@@ -29,8 +29,8 @@ struct RodView {
     float4* q;
     float4* qPrev;
     float4* omega;
-    float4* lamS;
-    float4* lamB;
+    float4* lamS;   // multipliers; null when each constraint is projected once
+    float4* lamB;   // per substep (one iteration: they start at zero)
     float4* force;
     float4* kin;
     float4* torque;
@@ -151,10 +151,12 @@ __device__ __forceinline__ void projectStretchAt(const RodView& V, int k, int i0
     A.m[1][1] += alpha.y;
     A.m[2][2] += alpha.z;
 
-    const V3 lam = v3(V.lamS[k]);
+    // no multiplier array: one iteration, so this projection is the
+    // constraint's only one of the substep and its multiplier starts at zero
+    const V3 lam = V.lamS ? v3(V.lamS[k]) : V3{0.0f, 0.0f, 0.0f};
     V3 dL;
     if (!solveSPD3(A, -(C + cwise(alpha, lam)), dL)) return;
-    V.lamS[k] = f4(lam + dL);
+    if (V.lamS) V.lamS[k] = f4(lam + dL);
 
     const V3 world = rotate(q, dL);
     addPos<COMP>(V, i0, -(world * (w0 / l)));
@@ -197,10 +199,10 @@ __device__ __forceinline__ void projectBendAt(const RodView& V, int k, int a, in
     A.m[1][1] += alpha.y;
     A.m[2][2] += alpha.z;
 
-    const V3 lam = v3(V.lamB[k]);
+    const V3 lam = V.lamB ? v3(V.lamB[k]) : V3{0.0f, 0.0f, 0.0f};
     V3 dL;
     if (!solveSPD3(A, -(C + cwise(alpha, lam)), dL)) return;
-    V.lamB[k] = f4(lam + dL);
+    if (V.lamB) V.lamB[k] = f4(lam + dL);
 
     if (norm2(iIa) > 0.0f) {
         const V3 g = (dL * -p.w - cross(im(p), dL)) * (1.0f / lbar);
