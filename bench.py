@@ -382,11 +382,12 @@ def run_served(capacity: float, seconds: float, seed: int, load: float, budget_g
 
 
 def measure_shapes(stream, fp32_peak: float) -> dict:
-    """The other named shapes, batched and plain, short timed runs on the same
-    GPU: the clamped 64-segment cantilever with a tip load (latency of one
-    rod), the 4096 x 64 driven grid over a floor, and the 3600-cable hook
-    sweep in mixed precision (compensated positions and frames, FP64 cone and
-    verdicts). Device time with CUDA events after 3 warm-up steps."""
+    """The other named shapes, batched (autotuned: for one short rod the tuner
+    picks one rod per CTA) and plain, short timed runs on the same GPU: the
+    clamped 64-segment cantilever with a tip load (latency of one rod), the
+    4096 x 64 driven grid over a floor, and the 3600-cable hook sweep in mixed
+    precision (compensated positions and frames, FP64 cone and verdicts).
+    Device time with CUDA events after 3 warm-up steps."""
     import torch
 
     import ropephysics_b200 as rp
@@ -399,10 +400,13 @@ def measure_shapes(stream, fp32_peak: float) -> dict:
                                  ("hook", W.hook(), mixed, 20)):
         seg_sub = wl.segment_substeps_per_step()
         rates = {}
+        tuning = None
         for label, strat in (("batched", rp.Strategy.BATCHED), ("plain", rp.Strategy.FUSED)):
             b = wl.make_batch(strat)
             b.set_precision(int(prec))
             b.set_stream(stream.cuda_stream)
+            if strat == rp.Strategy.BATCHED:  # as a user's batch would run: autotuned
+                tuning = b.autotune(wl.params, max_steps_per_launch=4)
             b.set_graph(True)
             b.step_many(wl.params, 3)
             b.step_many(wl.params, steps)
@@ -416,7 +420,7 @@ def measure_shapes(stream, fp32_peak: float) -> dict:
             rates[label] = (seg_sub / (ms / 1e3), ms)
             b.close()
         flops = FLOPS_PER_SEG_SUBSTEP.get(key, 890.5)
-        out[key] = {"workload": wl.name, "precision": int(prec), "unit": "segment-substeps/s",
+        out[key] = {"workload": wl.name, "precision": int(prec), "unit": "segment-substeps/s", "tuning": tuning,
                     "batched": rates["batched"][0], "plain": rates["plain"][0],
                     "speedup": rates["batched"][0] / rates["plain"][0],
                     "ms_per_step_batched": rates["batched"][1], "ms_per_step_plain": rates["plain"][1],
