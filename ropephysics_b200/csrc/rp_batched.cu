@@ -166,8 +166,8 @@ __device__ void countSelfByBlocks(const RodView& V, const SelfScratch& S, int nS
                     const float bound = cj.w + ck.w + twoR;
                     const float plim = bound * 1.001f + scaleSlack;
                     if (ddx * ddx + ddy * ddy + ddz * ddz > plim * plim) continue;
-                    const SegPair P = segmentPairNarrow(v3(V.x[V.sP0[j]]), v3(V.x[V.sP1[j]]),
-                                                        v3(V.x[V.sP0[k]]), v3(V.x[V.sP1[k]]), twoR);
+                    const SegPair P = segmentPairNarrow(v3(V.x[V.g->sP0[j]]), v3(V.x[V.g->sP1[j]]),
+                                                        v3(V.x[V.g->sP0[k]]), v3(V.x[V.g->sP1[k]]), twoR);
                     if (P.separation >= 0.0f) continue;
                     const int mult = bucketMultiplicity(cj, ck, cell, table);
                     if (mult) {
@@ -180,21 +180,22 @@ __device__ void countSelfByBlocks(const RodView& V, const SelfScratch& S, int nS
     }
 }
 
-// Everything a team needs about its rod beyond the shared arrays: the views
-// of its arrays, its scratch words and colour tables, its drive. Lane 0 writes
-// it once per rod into shared memory and every phase reads the fields it
-// uses, so the substep loop carries only the current phase's values in
-// registers (held in registers, these pointers alone filled a third of the
-// register file and pushed the constraint arithmetic into spills).
+// What a team needs about its rod beyond its shared-memory arrays: the fixed
+// global pointers, the colour tables, the drive, the self-contact scratch.
+// Lane 0 writes it once per rod into shared memory and every phase reads the
+// fields it uses, so the substep loop carries only the current phase's values
+// in registers (held in registers, these 64-bit pointers filled a third of
+// the register file and pushed the constraint arithmetic into spills). The
+// arrays in shared memory are not reached through it: pointers read back
+// from memory lose their address space, and every access through them
+// would be a generic load.
 struct TeamCtx {
-    RodView V;
-    SelfScratch S;
+    RodGlobals G;                   // the rod's fixed global pointers (V.g)
+    RodView V;                      // copies of the view and scratch for the
+    SelfScratch S;                  // separately compiled self-contact paths
     int32_t* cursor;                // hash placement cursors (table entries)
     int32_t* partial;               // scan partials, one per warp
     int32_t* numLevels;             // projection levels of the pool
-    unsigned long long* primMask;   // this substep's primitive cull
-    int32_t* touching;              // some segment pair touches this substep
-    float* red;                     // per-warp reduction rows, 8 floats each
     int32_t* lvlOrder;
     int32_t* lvlStart;
     int32_t* lvlOf;
@@ -327,26 +328,19 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
     const DTemplate T = A.tmpl[R.tmpl];
     const int nP = T.nP, nS = T.nS, nSt = T.nSt, nB = T.nB;
 
-    RodView Vb;  // built here, read through the shared context below
-#define V Vb
-    V.invMass = A.tInvMass + T.pOff;
-    V.invInertia = A.tInvInertia + T.sOff;
-    V.inertia = A.tInertia + T.sOff;
-    V.sP0 = A.tSP0 + T.stOff;
-    V.sP1 = A.tSP1 + T.stOff;
-    V.sSeg = A.tSSeg + T.stOff;
-    V.sComp = A.tSComp + T.stOff;
-    V.bA = A.tBA + T.bOff;
-    V.bB = A.tBB + T.bOff;
-    V.bComp = A.tBComp + T.bOff;
-    V.bRestD = A.tBRestD + T.bOff;
-    V.prims = A.prims + R.primOff;
+    TeamCtx& C = ctxs[teamIdx];
+    // The view of the rod's arrays lives in registers: its shared-memory
+    // arrays are addressed from `base`, so the compiler reaches them with
+    // shared-memory instructions through 32-bit addresses. The fixed global
+    // pointers (loads, template, primitives) sit in the team's context,
+    // reached through V.g.
+    RodView V;
+    V.g = &C.G;
     V.numPrims = R.numPrims;
     V.complianceScale = A.complianceScale[r];
     V.frictionScale = A.frictionScale[r];
     V.radius = R.radius;
     V.contactMargin = R.contactMargin;
-
     const RodLayout L = rodLayout(nP, nS, nSt, nB, R.numPrims, R.selfCollision, R.hashTableSize,
                                   R.selfCapacity, 1, COMP ? 1 : 0, A.slotsShared);
     V.q = reinterpret_cast<float4*>(base + L.q);
@@ -355,18 +349,13 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
     V.xPrev = reinterpret_cast<float4*>(base + L.xPrev);
     V.xComp = COMP ? reinterpret_cast<float4*>(base + L.xComp) : A.xComp + R.pOff;
     V.qComp = COMP ? reinterpret_cast<float4*>(base + L.qComp) : A.qComp + R.sOff;
-    // lean layout: loads and kinematic velocities stay in global memory
     V.v = reinterpret_cast<float4*>(base + L.v);
-    V.force = A.force + R.pOff;
-    V.kin = A.kinVel + R.pOff;
     V.omega = reinterpret_cast<float4*>(base + L.omega);
-    V.torque = A.torque + R.sOff;
     // multipliers: none at one iteration; else in global memory (L1/L2)
     V.lamS = A.iterations > 1 ? A.gLamS + R.stOff : nullptr;
     V.lamB = A.iterations > 1 ? A.gLamB + R.bOff : nullptr;
     V.slots = A.slotsShared ? reinterpret_cast<DSlot*>(base + L.slots) : A.gSlots + R.slotOff;
-    SelfScratch Sb;
-#define S Sb
+    SelfScratch S;
     S.centres = reinterpret_cast<float4*>(base + L.centres);
     S.segCount = reinterpret_cast<int32_t*>(base + L.selfInt);
     S.segStart = S.segCount + nSt;
@@ -380,18 +369,34 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
     S.live = misc + 1;
     S.overflow = misc + 2;
     S.blocks = reinterpret_cast<float4*>(base + L.blocks);
-#undef V
-#undef S
-    TeamCtx& C = ctxs[teamIdx];
+    int32_t* partial = misc + 4;  // one per warp of the team (up to 8)
+    int32_t* numLevels = misc + 3;
+    unsigned long long* primMask = reinterpret_cast<unsigned long long*>(misc + 12);
+    int32_t* touching = misc + 14;
+    float* red = reinterpret_cast<float*>(misc + 16);  // 8 floats per warp
     if (lane == 0) {
-        C.V = Vb;
-        C.S = Sb;
-        C.cursor = Sb.cellStart + (R.hashTableSize + 1);
-        C.partial = misc + 4;  // one per warp of the team (up to 8)
-        C.numLevels = misc + 3;
-        C.primMask = reinterpret_cast<unsigned long long*>(misc + 12);
-        C.touching = misc + 14;
-        C.red = reinterpret_cast<float*>(misc + 16);  // 8 floats per warp
+        RodGlobals& G = C.G;
+        G.invMass = A.tInvMass + T.pOff;
+        G.invInertia = A.tInvInertia + T.sOff;
+        G.inertia = A.tInertia + T.sOff;
+        G.sP0 = A.tSP0 + T.stOff;
+        G.sP1 = A.tSP1 + T.stOff;
+        G.sSeg = A.tSSeg + T.stOff;
+        G.sComp = A.tSComp + T.stOff;
+        G.bA = A.tBA + T.bOff;
+        G.bB = A.tBB + T.bOff;
+        G.bComp = A.tBComp + T.bOff;
+        G.bRestD = A.tBRestD + T.bOff;
+        G.prims = A.prims + R.primOff;
+        // lean layout: loads and kinematic velocities stay in global memory
+        G.force = A.force + R.pOff;
+        G.kin = A.kinVel + R.pOff;
+        G.torque = A.torque + R.sOff;
+        C.V = V;  // for the rarely run, separately compiled self-contact paths
+        C.S = S;
+        C.partial = partial;
+        C.numLevels = numLevels;
+        C.cursor = S.cellStart + (R.hashTableSize + 1);
         C.lvlOrder = C.cursor + (R.hashTableSize + 1);
         C.lvlStart = C.lvlOrder + (R.selfCapacity + 1);
         C.lvlOf = C.lvlStart + (R.selfCapacity + 1);
@@ -399,8 +404,8 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
         C.bOrder = A.tOrder + T.bOrderOff;
         C.sCol = A.tColorStart + T.sColorOff;
         C.bCol = A.tColorStart + T.bColorOff;
-        *C.numLevels = 0;
-        *C.primMask = ~0ull;
+        *numLevels = 0;
+        *primMask = ~0ull;
         // simulated time of this rod, advanced per step exactly as the
         // one-step-per-launch path advances rodTime[r]
         C.tRod = A.rodTime[r];
@@ -421,13 +426,6 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
         }
     }
     teamSync(team, teamIdx);
-    const RodView& V = C.V;
-    const SelfScratch& S = C.S;
-    int32_t* const& partial = C.partial;
-    int32_t* const& numLevels = C.numLevels;
-    unsigned long long* const& primMask = C.primMask;
-    int32_t* const& touching = C.touching;
-    float* const& red = C.red;
     const int* const& sOrder = C.sOrder;
     const int* const& bOrder = C.bOrder;
     const int* const& sCol = C.sCol;
@@ -467,8 +465,8 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
     const int stepsHere = A.stepsPerLaunch > 0 ? A.stepsPerLaunch : 1;
     for (int step = 0; step < stepsHere; ++step) {
         if (lane == 0) {
-            if (C.driveP >= 0) V.kin[C.driveP] = driveVelocityB(C.drive, C.tRod);
-            if (C.wayP >= 0) V.kin[C.wayP] = waypointVelocity(A.waypoints[r], C.wayStep + step);
+            if (C.driveP >= 0) V.g->kin[C.driveP] = driveVelocityB(C.drive, C.tRod);
+            if (C.wayP >= 0) V.g->kin[C.wayP] = waypointVelocity(A.waypoints[r], C.wayStep + step);
         }
         teamSync(team, teamIdx);
         for (int sub = 0; sub < A.substeps; ++sub) {
@@ -496,7 +494,7 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
                         float4 blo = make_float4(3.0e38f, 3.0e38f, 3.0e38f, 0.0f);
                         float4 bhi = make_float4(-3.0e38f, -3.0e38f, -3.0e38f, 0.0f);
                         if (j < nSt) {
-                            const int p0 = T.chain ? j : V.sP0[j], p1 = T.chain ? j + 1 : V.sP1[j];
+                            const int p0 = T.chain ? j : V.g->sP0[j], p1 = T.chain ? j + 1 : V.g->sP1[j];
                             const V3 a = v3(V.x[p0]), b = v3(V.x[p1]);
                             const float len = norm(b - a);
                             const V3 c = (a + b) * 0.5f;

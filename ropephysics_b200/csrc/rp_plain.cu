@@ -24,21 +24,21 @@ namespace rp {
 
 namespace {
 
-__device__ __forceinline__ RodView staticView(const DArgs& A, const DTemplate& T, const DRod& R,
-                                              int r) {
+__device__ __forceinline__ RodView staticView(const DArgs& A, const DTemplate& T, const DRod& R, int r,
+                                              RodGlobals& G) {
+    G.invMass = A.tInvMass + T.pOff;
+    G.invInertia = A.tInvInertia + T.sOff;
+    G.inertia = A.tInertia + T.sOff;
+    G.sP0 = A.tSP0 + T.stOff;
+    G.sP1 = A.tSP1 + T.stOff;
+    G.sSeg = A.tSSeg + T.stOff;
+    G.sComp = A.tSComp + T.stOff;
+    G.bA = A.tBA + T.bOff;
+    G.bB = A.tBB + T.bOff;
+    G.bComp = A.tBComp + T.bOff;
+    G.bRestD = A.tBRestD + T.bOff;
+    G.prims = A.prims + R.primOff;
     RodView V;
-    V.invMass = A.tInvMass + T.pOff;
-    V.invInertia = A.tInvInertia + T.sOff;
-    V.inertia = A.tInertia + T.sOff;
-    V.sP0 = A.tSP0 + T.stOff;
-    V.sP1 = A.tSP1 + T.stOff;
-    V.sSeg = A.tSSeg + T.stOff;
-    V.sComp = A.tSComp + T.stOff;
-    V.bA = A.tBA + T.bOff;
-    V.bB = A.tBB + T.bOff;
-    V.bComp = A.tBComp + T.bOff;
-    V.bRestD = A.tBRestD + T.bOff;
-    V.prims = A.prims + R.primOff;
     V.numPrims = R.numPrims;
     V.complianceScale = A.complianceScale[r];
     V.frictionScale = A.frictionScale[r];
@@ -60,7 +60,7 @@ __device__ __forceinline__ float4 driveVelocity(const DDrive& d, double t) {
 __device__ void buildSelfHashSerial(const RodView& V, const SelfScratch& S, int nSeg, int table) {
     float maxSegLen = 0.0f;
     for (int j = 0; j < nSeg; ++j) {
-        const V3 a = v3(V.x[V.sP0[j]]), b = v3(V.x[V.sP1[j]]);
+        const V3 a = v3(V.x[V.g->sP0[j]]), b = v3(V.x[V.g->sP1[j]]);
         S.centres[j] = f4((a + b) * 0.5f);
         const float len = norm(b - a);
         if (len > maxSegLen) maxSegLen = len;
@@ -90,7 +90,9 @@ __global__ void __launch_bounds__(128, 4) kPlainStep(DArgs A) {
     const int nP = T.nP, nS = T.nS, nSt = T.nSt, nB = T.nB;
     const int tid = threadIdx.x, nth = blockDim.x;
 
-    RodView V = staticView(A, T, R, r);
+    __shared__ RodGlobals sG;  // the rod's global pointers, read through V.g
+    RodGlobals G;
+    RodView V = staticView(A, T, R, r, G);
     SelfScratch S;
     float4* const gx = A.x + R.pOff;
     float4* const gv = A.v + R.pOff;
@@ -99,12 +101,12 @@ __global__ void __launch_bounds__(128, 4) kPlainStep(DArgs A) {
     if (GMEM) {
         V.x = gx;
         V.v = gv;
-        V.force = A.force + R.pOff;
-        V.kin = A.kinVel + R.pOff;
+        G.force = A.force + R.pOff;
+        G.kin = A.kinVel + R.pOff;
         V.xComp = A.xComp + R.pOff;
         V.q = gq;
         V.omega = gw;
-        V.torque = A.torque + R.sOff;
+        G.torque = A.torque + R.sOff;
         V.xPrev = A.gxPrev + R.pOff;
         V.qPrev = A.gqPrev + R.sOff;
         V.lamS = A.gLamS + R.stOff;
@@ -123,12 +125,12 @@ __global__ void __launch_bounds__(128, 4) kPlainStep(DArgs A) {
         V.q = reinterpret_cast<float4*>(smem + L.q);
         V.qPrev = reinterpret_cast<float4*>(smem + L.qPrev);
         V.omega = reinterpret_cast<float4*>(smem + L.omega);
-        V.torque = reinterpret_cast<float4*>(smem + L.torque);
+        G.torque = reinterpret_cast<float4*>(smem + L.torque);
         V.x = reinterpret_cast<float4*>(smem + L.x);
         V.xPrev = reinterpret_cast<float4*>(smem + L.xPrev);
         V.v = reinterpret_cast<float4*>(smem + L.v);
-        V.force = reinterpret_cast<float4*>(smem + L.force);
-        V.kin = reinterpret_cast<float4*>(smem + L.kin);
+        G.force = reinterpret_cast<float4*>(smem + L.force);
+        G.kin = reinterpret_cast<float4*>(smem + L.kin);
         V.xComp = reinterpret_cast<float4*>(smem + L.xComp);
         V.lamS = reinterpret_cast<float4*>(smem + L.lamS);
         V.lamB = reinterpret_cast<float4*>(smem + L.lamB);
@@ -142,6 +144,9 @@ __global__ void __launch_bounds__(128, 4) kPlainStep(DArgs A) {
         S.overflow = reinterpret_cast<int32_t*>(smem + L.misc) + 2;
     }
     V.qComp = A.qComp + R.sOff;  // compensated frames: global in both forms
+    if (tid == 0) sG = G;
+    __syncthreads();
+    V.g = &sG;
     S.sorted = S.cellOf + nSt;
     S.segCount = S.sorted + nSt;
     S.segStart = S.segCount + nSt;
@@ -175,17 +180,17 @@ __global__ void __launch_bounds__(128, 4) kPlainStep(DArgs A) {
         for (int i = tid; i < nP; i += nth) {
             V.x[i] = gx[i];
             V.v[i] = gv[i];
-            V.force[i] = gf[i];
-            V.kin[i] = i == driveP ? driveV : gk[i];
+            G.force[i] = gf[i];
+            G.kin[i] = i == driveP ? driveV : gk[i];
             if (COMP) V.xComp[i] = gc[i];
         }
         for (int j = tid; j < nS; j += nth) {
             V.q[j] = gq[j];
             V.omega[j] = gw[j];
-            V.torque[j] = gt[j];
+            G.torque[j] = gt[j];
         }
     } else if (driveP >= 0 && tid == 0) {
-        V.kin[driveP] = driveV;
+        G.kin[driveP] = driveV;
     }
     __syncthreads();
 

@@ -21,23 +21,15 @@
 
 namespace rp {
 
-struct RodView {
-    // dynamic state (shared or global memory)
-    float4* x;
-    float4* xPrev;
-    float4* v;
-    float4* q;
-    float4* qPrev;
-    float4* omega;
-    float4* lamS;   // multipliers; null when each constraint is projected once
-    float4* lamB;   // per substep (one iteration: they start at zero)
+// What a substep reads from global memory through pointers that stay fixed
+// for the whole step: the rod's loads and kinematic velocities, its
+// template's rest data and topology, its world's primitives. The kernels keep
+// one of these per rod in shared memory and reach it through RodView::g, so
+// the substep loop does not hold these pointers in registers.
+struct RodGlobals {
     float4* force;
     float4* kin;
     float4* torque;
-    float4* xComp;  // Kahan compensation (compensated precision only)
-    float4* qComp;  // frames' Kahan compensation (compensated precision only)
-    DSlot* slots;
-    // static template data (global memory, read-only)
     const float* invMass;
     const float4* invInertia;
     const float4* inertia;
@@ -50,6 +42,22 @@ struct RodView {
     const float4* bComp;
     const float4* bRestD;
     const DPrim* prims;
+};
+
+struct RodView {
+    // dynamic state (shared or global memory)
+    float4* x;
+    float4* xPrev;
+    float4* v;
+    float4* q;
+    float4* qPrev;
+    float4* omega;
+    float4* lamS;   // multipliers; null when each constraint is projected once
+    float4* lamB;   // per substep (one iteration: they start at zero)
+    float4* xComp;  // Kahan compensation (compensated precision only)
+    float4* qComp;  // frames' Kahan compensation (compensated precision only)
+    DSlot* slots;
+    const RodGlobals* g;  // loads, template data, primitives (global memory)
     int numPrims;
     float complianceScale;
     float frictionScale;
@@ -132,11 +140,11 @@ __device__ __forceinline__ void renormalizeFrameComp(const RodView& V, int j) {
 // passes sP0[k], sP1[k], sSeg[k], or k, k+1, k for a chain).
 template <bool COMP>
 __device__ __forceinline__ void projectStretchAt(const RodView& V, int k, int i0, int i1, int j, float invH2) {
-    const float w0 = V.invMass[i0], w1 = V.invMass[i1];
-    const V3 iI = v3(V.invInertia[j]);
+    const float w0 = V.g->invMass[i0], w1 = V.g->invMass[i1];
+    const V3 iI = v3(V.g->invInertia[j]);
     if (w0 == 0.0f && w1 == 0.0f && norm2(iI) == 0.0f) return;
 
-    const float4 sc = V.sComp[k];
+    const float4 sc = V.g->sComp[k];
     const float l = sc.w;
     const Q4 q = q4(V.q[j]);
     V3 d = v3(V.x[i1]) - v3(V.x[i0]);
@@ -172,22 +180,22 @@ __device__ __forceinline__ void projectStretchAt(const RodView& V, int k, int i0
 
 template <bool COMP>
 __device__ __forceinline__ void projectStretchOne(const RodView& V, int k, float invH2) {
-    projectStretchAt<COMP>(V, k, V.sP0[k], V.sP1[k], V.sSeg[k], invH2);
+    projectStretchAt<COMP>(V, k, V.g->sP0[k], V.g->sP1[k], V.g->sSeg[k], invH2);
 }
 
 // Bend/twist constraint k between frames a and b (bA[k], bB[k], or k, k+1
 // for a chain's real frames).
 template <bool COMP>
 __device__ __forceinline__ void projectBendAt(const RodView& V, int k, int a, int b, float invH2) {
-    const V3 iIa = v3(V.invInertia[a]), iIb = v3(V.invInertia[b]);
+    const V3 iIa = v3(V.g->invInertia[a]), iIb = v3(V.g->invInertia[b]);
     if (norm2(iIa) == 0.0f && norm2(iIb) == 0.0f) return;
 
-    const float4 bc = V.bComp[k];
+    const float4 bc = V.g->bComp[k];
     const float lbar = bc.w;
     const Q4 qa = q4(V.q[a]);
     const Q4 qb = q4(V.q[b]);
     const Q4 p = sameHemisphereId(qmul(conj(qa), qb));
-    const V3 C = im(p) * (2.0f / lbar) - v3(V.bRestD[k]);
+    const V3 C = im(p) * (2.0f / lbar) - v3(V.g->bRestD[k]);
 
     const M3 skewPv = mskew(im(p));
     const M3 Ja = mscale(madd(midentity(-p.w), skewPv), 1.0f / lbar);
@@ -222,7 +230,7 @@ __device__ __forceinline__ void projectBendAt(const RodView& V, int k, int a, in
 
 template <bool COMP>
 __device__ __forceinline__ void projectBendOne(const RodView& V, int k, float invH2) {
-    projectBendAt<COMP>(V, k, V.bA[k], V.bB[k], invH2);
+    projectBendAt<COMP>(V, k, V.g->bA[k], V.g->bB[k], invH2);
 }
 
 // ---------------------------------------------------------------- world contacts
@@ -270,7 +278,7 @@ __device__ __forceinline__ void keepSlot(const RodView& V, int i, DSlot& c) {
 template <bool COMP>
 __device__ __forceinline__ void generateSlots(const RodView& V, int i, bool regenerate) {
     const int base = i * V.numPrims;
-    const float w = V.invMass[i];
+    const float w = V.g->invMass[i];
     for (int k = 0; k < V.numPrims; ++k) {
         DSlot& c = V.slots[base + k];
         c.lambdaN = 0.0f;
@@ -281,7 +289,7 @@ __device__ __forceinline__ void generateSlots(const RodView& V, int i, bool rege
         }
         c.state = 0;
         if (w == 0.0f) continue;  // pinned: cannot respond
-        generateSlot<COMP>(V, i, loadPrim(V.prims[k]), c);
+        generateSlot<COMP>(V, i, loadPrim(V.g->prims[k]), c);
     }
 }
 
@@ -300,7 +308,7 @@ __device__ __forceinline__ unsigned long long primitivesNearBox(const RodView& V
                         1e-5f * (fabsf(c.x) + fabsf(c.y) + fabsf(c.z) + e.x + e.y + e.z);
     unsigned long long mask = 0ull;
     for (int k = 0; k < V.numPrims && k < 64; ++k) {
-        const PrimF P = loadPrim(V.prims[k]);
+        const PrimF P = loadPrim(V.g->prims[k]);
         bool near;
         if (P.type == 0) {
             const float s = dot(c - P.a, P.n) -
@@ -331,7 +339,7 @@ template <bool COMP>
 __device__ __forceinline__ void generateSlotsMasked(const RodView& V, int i, bool regenerate,
                                                     unsigned long long mask) {
     const int base = i * V.numPrims;
-    const float w = V.invMass[i];
+    const float w = V.g->invMass[i];
     for (int k = 0; k < V.numPrims; ++k) {
         if (!((mask >> k) & 1ull)) continue;
         DSlot& c = V.slots[base + k];
@@ -343,7 +351,7 @@ __device__ __forceinline__ void generateSlotsMasked(const RodView& V, int i, boo
         }
         c.state = 0;
         if (w == 0.0f) continue;
-        generateSlot<COMP>(V, i, loadPrim(V.prims[k]), c);
+        generateSlot<COMP>(V, i, loadPrim(V.g->prims[k]), c);
     }
 }
 
@@ -352,7 +360,7 @@ __device__ __forceinline__ void generateSlotsMasked(const RodView& V, int i, boo
 // double-precision cone test (RP_PRECISION_FP64_CONE).
 template <bool COMP, bool FP64>
 __device__ __forceinline__ void projectSlots(const RodView& V, int i, unsigned long long mask) {
-    const float w = V.invMass[i];
+    const float w = V.g->invMass[i];
     if (w <= 0.0f) return;
     const int base = i * V.numPrims;
     for (int k = 0; k < V.numPrims; ++k) {
@@ -460,7 +468,7 @@ __device__ __forceinline__ void querySelfSegment(const RodView& V, const SelfScr
         const float4 cj4 = S.centres[j];
         const V3 cj = v3(cj4);
         const int cx = cellCoord(cj.x, cell), cy = cellCoord(cj.y, cell), cz = cellCoord(cj.z, cell);
-        const V3 a0 = v3(V.x[V.sP0[j]]), a1 = v3(V.x[V.sP1[j]]);
+        const V3 a0 = v3(V.x[V.g->sP0[j]]), a1 = v3(V.x[V.g->sP1[j]]);
         const float twoR = 2.0f * V.radius;
         const float scaleSlack = 1e-6f * (1.0f + fabsf(cj.x) + fabsf(cj.y) + fabsf(cj.z));
         for (int dz = -1; dz <= 1; ++dz)
@@ -478,7 +486,7 @@ __device__ __forceinline__ void querySelfSegment(const RodView& V, const SelfScr
                             const float lim = bound * 1.001f + scaleSlack;
                             if (ddx * ddx + ddy * ddy + ddz * ddz > lim * lim) continue;
                         }
-                        const V3 b0 = v3(V.x[V.sP0[k]]), b1 = v3(V.x[V.sP1[k]]);
+                        const V3 b0 = v3(V.x[V.g->sP0[k]]), b1 = v3(V.x[V.g->sP1[k]]);
                         const SegPair P = segmentPairNarrow(a0, a1, b0, b1, twoR);
                         if (P.separation >= 0.0f) continue;
                         const float u = P.u, w = P.w, dist = P.dist, separation = P.separation;
@@ -491,10 +499,10 @@ __device__ __forceinline__ void querySelfSegment(const RodView& V, const SelfScr
                         c.nx = n.x;
                         c.ny = n.y;
                         c.nz = n.z;
-                        c.idx[0] = V.sP0[j];
-                        c.idx[1] = V.sP1[j];
-                        c.idx[2] = V.sP0[k];
-                        c.idx[3] = V.sP1[k];
+                        c.idx[0] = V.g->sP0[j];
+                        c.idx[1] = V.g->sP1[j];
+                        c.idx[2] = V.g->sP0[k];
+                        c.idx[3] = V.g->sP1[k];
                         c.weight[0] = 1.0f - u;
                         c.weight[1] = u;
                         c.weight[2] = -(1.0f - w);
@@ -593,7 +601,7 @@ __device__ __forceinline__ int buildProjectionColors(const DSelf* pool, int live
 template <bool COMP>
 __device__ __forceinline__ void projectSelf(const RodView& V, DSelf& c) {
     float wEff = 0.0f;
-    for (int m = 0; m < 4; ++m) wEff += c.weight[m] * c.weight[m] * V.invMass[c.idx[m]];
+    for (int m = 0; m < 4; ++m) wEff += c.weight[m] * c.weight[m] * V.g->invMass[c.idx[m]];
     if (wEff <= 0.0f) return;
     const V3 n{c.nx, c.ny, c.nz};
 
@@ -605,7 +613,7 @@ __device__ __forceinline__ void projectSelf(const RodView& V, DSelf& c) {
     c.lambdaN = clamped;
     if (dLambda != 0.0f)
         for (int m = 0; m < 4; ++m)
-            addPos<COMP>(V, c.idx[m], n * (V.invMass[c.idx[m]] * c.weight[m] * dLambda));
+            addPos<COMP>(V, c.idx[m], n * (V.g->invMass[c.idx[m]] * c.weight[m] * dLambda));
 
     if (c.friction <= 0.0f || c.lambdaN <= 0.0f) return;
 
@@ -623,7 +631,7 @@ __device__ __forceinline__ void projectSelf(const RodView& V, DSelf& c) {
     c.applied += capped;
     const V3 correction = tangential * (-capped / slide);
     for (int m = 0; m < 4; ++m)
-        addPos<COMP>(V, c.idx[m], correction * (V.invMass[c.idx[m]] * c.weight[m] / wEff));
+        addPos<COMP>(V, c.idx[m], correction * (V.g->invMass[c.idx[m]] * c.weight[m] / wEff));
 }
 
 // ---------------------------------------------------------------- predict / finish
@@ -631,12 +639,12 @@ __device__ __forceinline__ void projectSelf(const RodView& V, DSelf& c) {
 template <bool COMP>
 __device__ __forceinline__ void predictParticle(const RodView& V, int i, float h, V3 g) {
     V.xPrev[i] = COMP ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : V.x[i];
-    const float w = V.invMass[i];
+    const float w = V.g->invMass[i];
     if (w == 0.0f) {
-        addPos<COMP>(V, i, v3(V.kin[i]) * h);  // prescribed motion
+        addPos<COMP>(V, i, v3(V.g->kin[i]) * h);  // prescribed motion
         return;
     }
-    const V3 vn = v3(V.v[i]) + (g + v3(V.force[i]) * w) * h;
+    const V3 vn = v3(V.v[i]) + (g + v3(V.g->force[i]) * w) * h;
     V.v[i] = f4(vn);
     addPos<COMP>(V, i, vn * h);
 }
@@ -646,13 +654,13 @@ __device__ __forceinline__ void predictFrame(const RodView& V, int j, float h) {
     const float4 qs = V.q[j];
     // compensated: the substep's accumulated rotation starts at identity
     V.qPrev[j] = COMP ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : qs;
-    const V3 iI = v3(V.invInertia[j]);
+    const V3 iI = v3(V.g->invInertia[j]);
     if (norm2(iI) == 0.0f) return;
     if (COMP) renormalizeFrameComp(V, j);  // once per substep, in FP64
     const V3 w = v3(V.omega[j]);
     const Q4 q = q4(V.q[j]);
-    const V3 tau = rotateInv(q, v3(V.torque[j]));
-    const V3 wn = w + cwise(iI, tau - cross(w, cwise(v3(V.inertia[j]), w))) * h;
+    const V3 tau = rotateInv(q, v3(V.g->torque[j]));
+    const V3 wn = w + cwise(iI, tau - cross(w, cwise(v3(V.g->inertia[j]), w))) * h;
     V.omega[j] = f4(wn);
     if (COMP)
         rotateFrameComp(V, j, wn * (0.5f * h));
@@ -662,8 +670,8 @@ __device__ __forceinline__ void predictFrame(const RodView& V, int j, float h) {
 
 template <bool COMP>
 __device__ __forceinline__ void finishParticle(const RodView& V, int i, float h, float linDecay) {
-    if (V.invMass[i] == 0.0f) {
-        V.v[i] = V.kin[i];
+    if (V.g->invMass[i] == 0.0f) {
+        V.v[i] = V.g->kin[i];
         return;
     }
     const V3 d = dispOf<COMP>(V, i);
@@ -672,7 +680,7 @@ __device__ __forceinline__ void finishParticle(const RodView& V, int i, float h,
 
 template <bool COMP>
 __device__ __forceinline__ void finishFrame(const RodView& V, int j, float h, float angDecay) {
-    if (norm2(v3(V.invInertia[j])) == 0.0f) {
+    if (norm2(v3(V.g->invInertia[j])) == 0.0f) {
         V.omega[j] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         return;
     }
