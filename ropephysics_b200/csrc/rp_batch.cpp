@@ -178,6 +178,12 @@ static rp_status createImpl(const rp_rod_desc* const* rods, int numRods, const r
             R.numPrims = W.num_primitives;
             R.contactMargin = float(W.contact_margin_radii * d->material.radius);
             if (W.self_collision) {
+                // the batched kernel reuses a rod's 2 nSt sort ints as one int
+                // per particle when it builds the projection levels
+                if (strategy == RP_STRATEGY_BATCHED && T.nP > 2 * T.nSt)
+                    return guard(fail(RP_ERR_INVALID, "rod " + std::to_string(r) +
+                                                          ": self-collision in the batched strategy needs "
+                                                          "particles <= 2 x stretch constraints"));
                 R.selfCollision = 1;
                 auto key = std::make_pair(t, W.self_skip);
                 auto g = gapCache.find(key);
@@ -205,6 +211,8 @@ static rp_status createImpl(const rp_rod_desc* const* rods, int numRods, const r
         b->anySelf = b->anySelf || R.selfCollision;
         const rp::RodLayout L = rp::rodLayout(T.nP, T.nS, T.nSt, T.nB, R.numPrims, R.selfCollision,
                                               R.hashTableSize, R.selfCapacity);
+        if (!rp::rodLayoutAligned(L))
+            return guard(fail(RP_ERR_INVALID, "internal: a rod's shared-memory layout is not 16-byte aligned"));
         maxLayout = std::max(maxLayout, size_t(L.bytes));
         b->rods[r] = R;
         b->tmplNP[r] = T.nP;
@@ -381,13 +389,16 @@ rp_status buildBatchedPlan(rp_batch* b, const Tune& tune, int precision) {
     // rods); otherwise they stay in global memory.
     size_t maxSmem = rpx::planGroups(ids, b->rods.data(), b->tmpls.data(), cta, tune.pairsPerThread, comp,
                                      order, groups, false);
+    if (maxSmem == rpx::kMisaligned)
+        return fail(RP_ERR_INVALID, "internal: a rod's shared-memory layout is not 16-byte aligned");
     int slotsShared = 0;
     if (b->maxPrims > 0) {
         std::vector<int32_t> order2, groups2;
         const size_t smem2 = rpx::planGroups(ids, b->rods.data(), b->tmpls.data(), cta, tune.pairsPerThread,
                                              comp, order2, groups2, true);
         int per1 = 0, per2 = 0;
-        if (smem2 + fixed <= optin && rp::batchedReserveSmem(std::max(smem2, maxSmem)) == cudaSuccess &&
+        if (smem2 != rpx::kMisaligned && smem2 + fixed <= optin &&
+            rp::batchedReserveSmem(std::max(smem2, maxSmem)) == cudaSuccess &&
             rp::batchedOccupancy(cta, maxSmem, precision, &per1) == cudaSuccess &&
             rp::batchedOccupancy(cta, smem2, precision, &per2) == cudaSuccess && per2 >= per1 && per2 >= 1) {
             maxSmem = smem2;

@@ -52,6 +52,7 @@ struct TemplateHost {
 };
 void makeTemplate(const rp_rod_desc* d, TemplateHost& out);
 int teamThreads(int nSt, int pairsPerThread);
+constexpr size_t kMisaligned = ~size_t(0);
 size_t planGroups(const std::vector<int32_t>& rodIds, const rp::DRod* rods, const rp::DTemplate* tmpls,
                   int cta, int pairsPerThread, bool comp, std::vector<int32_t>& order,
                   std::vector<int32_t>& groups, bool slotsShared = false);

@@ -199,7 +199,9 @@ int teamThreads(int nSt, int pairsPerThread) {
     return std::max(32, std::min(256, t));
 }
 
-// Length-sorted groups for the batched kernel. `order` receives the rod ids
+// Length-sorted groups for the batched kernel (kMisaligned if a rod's layout
+// would break the 16-byte alignment its rows and bulk copies need: refused
+// on the host, never launched). `order` receives the rod ids
 // longest first (stable), `groups` four ints per group: first index into
 // `order`, rod count, team size, shared bytes. Returns the largest group's
 // shared bytes.
@@ -227,6 +229,7 @@ size_t planGroups(const std::vector<int32_t>& rodIds, const rp::DRod* rods, cons
             const rp::RodLayout L = rp::rodLayout(T.nP, T.nS, T.nSt, T.nB, R.numPrims, R.selfCollision,
                                                   R.hashTableSize, R.selfCapacity, 1, comp ? 1 : 0,
                                                   slotsShared ? 1 : 0);
+            if (!rp::rodLayoutAligned(L)) return kMisaligned;
             smem += size_t(L.bytes);
             ++cnt;
         }

@@ -115,7 +115,7 @@ RP_HD inline RodLayout rodLayout(int32_t nP, int32_t nS, int32_t nSt, int32_t nB
         // the projection levels (touched only while a pair touches) and the
         // pool live in global memory
         L.centres = o; o += 16 * nSt;
-        L.selfInt = o; o += 8 * nSt;  // per-segment count and start
+        L.selfInt = o; o += rpAlign16(8 * nSt);  // per-segment count and start
         L.hash = L.pool = L.levels = -1;
         L.blocks = o;  o += 32 * ((nSt + 7) / 8);
     } else {
@@ -124,6 +124,18 @@ RP_HD inline RodLayout rodLayout(int32_t nP, int32_t nS, int32_t nSt, int32_t nB
     }
     L.bytes = o;
     return L;
+}
+
+// Every section starts on a 16-byte boundary and the total is a multiple of
+// 16 (float4 rows, bulk copies, and the next rod's slice of a group all need
+// it); -1 marks a section the layout does not hold.
+RP_HD inline bool rodLayoutAligned(const RodLayout& L) {
+    const int32_t s[] = {L.q, L.qPrev, L.omega, L.torque, L.x, L.xPrev, L.v, L.force, L.kin, L.xComp, L.qComp,
+                         L.lamS, L.lamB, L.slots, L.centres, L.selfInt, L.misc, L.hash, L.pool, L.levels,
+                         L.blocks, L.bytes};
+    for (int32_t v : s)
+        if (v != -1 && (v & 15) != 0) return false;
+    return true;
 }
 
 }  // namespace rp

@@ -316,6 +316,10 @@ bool rp_server::plan() {
     for (auto& rq : running) ids.insert(ids.end(), rq->rodIds.begin(), rq->rodIds.end());
     const bool comp = (cfg.precision & RP_PRECISION_COMPENSATED) != 0;
     smem = rpx::planGroups(ids, hRods.data(), hTmpls.data(), 256, 1, comp, order, groups);
+    if (smem == rpx::kMisaligned) {
+        workerError = "internal: a rod's shared-memory layout is not 16-byte aligned";
+        return false;
+    }
     if (smem + rp::batchedStaticSmem() + 64 > rpx::optinSmem(device)) {
         workerError = "a rod group exceeds shared memory";
         return false;
@@ -662,6 +666,11 @@ rp_status rp_server_submit(rp_server* s, const rp_request* r, uint64_t* id) {
             R.numPrims = W.num_primitives;
             R.contactMargin = float(W.contact_margin_radii * d->material.radius);
             if (W.self_collision) {
+                // the batched kernel reuses a rod's 2 nSt sort ints as one int
+                // per particle when it builds the projection levels
+                if (T.nP > 2 * T.nSt)
+                    return fail(RP_ERR_INVALID, "rod " + std::to_string(i) +
+                                                    ": self-collision needs particles <= 2 x stretch constraints");
                 R.selfCollision = 1;
                 R.selfGap = rpx::selfGap(d, W.self_skip);
                 R.selfFriction = float(W.self_friction);
