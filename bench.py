@@ -507,13 +507,15 @@ def run_ours(args):
     batch.synchronize()
     # the end-to-end twin: the same rods, advanced to the state the timed
     # region starts from (every launch shape gives bitwise the same steps)
-    twin = None
+    twins = []
     if not args.no_e2e:
-        twin = wl.make_batch(rp.Strategy.BATCHED)
-        twin.set_stream(stream.cuda_stream)
-        twin.set_tuning(tuning["cta_threads"], tuning["pairs_per_thread"], 1)
-        twin.step_many(p, args.warmup + args.steps)
-        twin.synchronize()
+        for _ in range(2):  # pipelined and serial end-to-end runs
+            twin = wl.make_batch(rp.Strategy.BATCHED)
+            twin.set_stream(stream.cuda_stream)
+            twin.set_tuning(tuning["cta_threads"], tuning["pairs_per_thread"], 1)
+            twin.step_many(p, args.warmup + args.steps)
+            twin.synchronize()
+            twins.append(twin)
 
     # ---- device-resident throughput (value) ----
     barrier(world_size)
@@ -533,39 +535,72 @@ def run_ours(args):
 
     # ---- end to end through the public API with pinned host buffers ----
     # Every step: the kinematic velocities in (host -> device), one step, the
-    # positions, frames and contact states out (device -> host), then a host
-    # synchronize. Same rods and same starting state as the timed region.
+    # positions, frames and contact states out (device -> host). Same rods and
+    # same starting state as the timed region (twin batches). Two ways:
+    #   pipelined  the copies ride a second stream (the overlapped copy calls)
+    #              and the host takes step k's results while step k+1 runs;
+    #              input and output host buffers are double-buffered
+    #   serial     copies on the batch's stream and a host synchronize after
+    #              every step; per-phase event times
     e2e = None
-    if twin is not None:
-        nbytes = {k: twin.state_bytes(k) for k in (twin.POSITIONS, twin.FRAMES, twin.CONTACTS)}
-        h2d = 16 * twin.total_particles
-        kin = torch.zeros(twin.total_particles * 4, dtype=torch.float32).pin_memory()
-        outs = {k: torch.empty(max(1, n), dtype=torch.uint8).pin_memory() for k, n in nbytes.items()}
+    if twins:
+        nbytes = {k: twins[0].state_bytes(k) for k in (twins[0].POSITIONS, twins[0].FRAMES, twins[0].CONTACTS)}
+        h2d = 16 * twins[0].total_particles
+        d2h = int(sum(nbytes.values()))
+        kin = [torch.zeros(twins[0].total_particles * 4, dtype=torch.float32).pin_memory() for _ in range(2)]
+        outs = [{k: torch.empty(max(1, n), dtype=torch.uint8).pin_memory() for k, n in nbytes.items()}
+                for _ in range(2)]
+        # pipelined
+        tw = twins[0]
+        copy = torch.cuda.Stream()
+        tw.set_copy_stream(copy.cuda_stream)
+        done = [torch.cuda.Event() for _ in range(args.steps)]
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier(world_size)
+        torch.cuda.synchronize()
+        t0.record(stream)
+        for k in range(args.steps):
+            tw.write_state_overlapped(tw.KINEMATIC, kin[k % 2].data_ptr(), h2d)
+            tw.step(p)
+            for what, n in nbytes.items():
+                if n:
+                    tw.read_state_overlapped(what, outs[k % 2][what].data_ptr(), n)
+            done[k].record(copy)
+            if k >= 1:
+                done[k - 1].synchronize()  # step k-1's results are in host memory
+        t1.record(copy)
+        t1.synchronize()
+        pipe_s = max_over_ranks(t0.elapsed_time(t1) / 1e3, world_size)
+        tw.close()
+        # serial
+        tw = twins[1]
         ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
         barrier(world_size)
         torch.cuda.synchronize()
         for k in range(args.steps):
             ev[k][0].record(stream)
-            twin.write_state_async(twin.KINEMATIC, kin.data_ptr(), h2d)
+            tw.write_state_async(tw.KINEMATIC, kin[0].data_ptr(), h2d)
             ev[k][1].record(stream)
-            twin.step(p)
+            tw.step(p)
             ev[k][2].record(stream)
             for what, n in nbytes.items():
                 if n:
-                    twin.read_state_async(what, outs[what].data_ptr(), n)
+                    tw.read_state_async(what, outs[0][what].data_ptr(), n)
             ev[k][3].record(stream)
-            twin.synchronize()
+            tw.synchronize()
         phase = [sum(ev[k][i].elapsed_time(ev[k][i + 1]) for k in range(args.steps)) / args.steps
                  for i in range(3)]
-        e2e_s = max_over_ranks(ev[0][0].elapsed_time(ev[-1][3]) / 1e3, world_size)
-        d2h = int(sum(nbytes.values()))
-        e2e = {"value": seg_sub * args.steps * world_size / e2e_s, "unit": "segment-substeps/s",
+        serial_s = max_over_ranks(ev[0][0].elapsed_time(ev[-1][3]) / 1e3, world_size)
+        tw.close()
+        e2e = {"value": seg_sub * args.steps * world_size / pipe_s, "unit": "segment-substeps/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-               "ms_per_step": e2e_s * 1e3 / args.steps,
-               "h2d_ms": phase[0], "step_ms": phase[1], "d2h_ms": phase[2],
-               "h2d_gbs": h2d / phase[0] / 1e6, "d2h_gbs": d2h / phase[2] / 1e6,
-               "start": "the timed region's starting state (twin batch)"}
-        twin.close()
+               "ms_per_step": pipe_s * 1e3 / args.steps,
+               "how": "pipelined: inputs and outputs of every step over the host link on a copy stream "
+                      "(rp_batch_*_state_overlapped), results of step k taken by the host while step k+1 runs",
+               "serial": {"value": seg_sub * args.steps * world_size / serial_s,
+                          "ms_per_step": serial_s * 1e3 / args.steps, "h2d_ms": phase[0], "step_ms": phase[1],
+                          "d2h_ms": phase[2], "h2d_gbs": h2d / phase[0] / 1e6, "d2h_gbs": d2h / phase[2] / 1e6},
+               "start": "the timed region's starting state (twin batches)"}
 
     # ---- plain one-rod-per-CTA step on the same batch (batched vs plain) ----
     plain_rate = None

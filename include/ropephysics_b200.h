@@ -424,6 +424,22 @@ enum { RP_STATE_POSITIONS = 0, RP_STATE_FRAMES = 1, RP_STATE_CONTACTS = 2, RP_ST
 rp_status rp_batch_read_state_async(rp_batch* batch, int32_t what, void* dst, int64_t bytes);
 rp_status rp_batch_write_state_async(rp_batch* batch, int32_t what, const void* src, int64_t bytes);
 
+/* Overlapped copies (no reference counterpart): the same arrays as
+ * rp_batch_read_state_async / rp_batch_write_state_async, but the bytes cross
+ * the host link on the caller's copy stream (rp_batch_set_copy_stream, a
+ * cudaStream_t) while later steps run on the batch's stream. A read first
+ * copies the rows on the device into a staging buffer the batch owns (after
+ * the work queued so far on the batch's stream, a few tens of microseconds),
+ * then to `dst` on the copy stream; a write lands in a staging buffer on the
+ * copy stream and is moved into place on the batch's stream before the next
+ * step. Host buffers must stay valid until the copy stream has passed the
+ * copy (record and wait an event on it); reading the same array again, or
+ * writing again, waits on the device for the previous copy out of (into) the
+ * staging buffer. The first call per array allocates its staging buffer. */
+rp_status rp_batch_set_copy_stream(rp_batch* batch, void* cuda_stream);
+rp_status rp_batch_read_state_overlapped(rp_batch* batch, int32_t what, void* dst, int64_t bytes);
+rp_status rp_batch_write_state_overlapped(rp_batch* batch, int32_t what, const void* src, int64_t bytes);
+
 /* Per (rod, particle, primitive) contact state at the end of the last step,
  * RP_CONTACT_*; layout rod-major: (particle_offset(rod) + i) * prims + k where
  * prims is the rod's primitive count. Returns the total slot count in *count. */

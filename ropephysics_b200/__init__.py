@@ -609,6 +609,15 @@ class Batch:
     def read_state_async(self, what: int, dst_ptr: int, nbytes: int):
         _check(lib().rp_batch_read_state_async(self._h, what, C.c_void_p(dst_ptr), nbytes))
 
+    def set_copy_stream(self, stream_ptr: int):
+        _check(lib().rp_batch_set_copy_stream(self._h, C.c_void_p(stream_ptr)))
+
+    def read_state_overlapped(self, what: int, dst_ptr: int, nbytes: int):
+        _check(lib().rp_batch_read_state_overlapped(self._h, what, C.c_void_p(dst_ptr), nbytes))
+
+    def write_state_overlapped(self, what: int, src_ptr: int, nbytes: int):
+        _check(lib().rp_batch_write_state_overlapped(self._h, what, C.c_void_p(src_ptr), nbytes))
+
     def write_state_async(self, what: int, src_ptr: int, nbytes: int):
         _check(lib().rp_batch_write_state_async(self._h, what, C.c_void_p(src_ptr), nbytes))
 

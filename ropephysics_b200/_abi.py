@@ -151,6 +151,9 @@ SIGNATURES = {
     "rp_batch_evaluate_harness": (i32, [vp, P(HarnessBoard), P(HarnessOutcome), i32]),
     "rp_batch_read_state_async": (i32, [vp, i32, vp, i64]),
     "rp_batch_write_state_async": (i32, [vp, i32, vp, i64]),
+    "rp_batch_set_copy_stream": (i32, [vp, vp]),
+    "rp_batch_read_state_overlapped": (i32, [vp, i32, vp, i64]),
+    "rp_batch_write_state_overlapped": (i32, [vp, i32, vp, i64]),
     "rp_batch_read_contact_states": (i32, [vp, P(u8), i64, P(i64)]),
     "rp_batch_read_self_contacts": (i32, [vp, i32, P(i32), i32, P(i32)]),
     "rp_batch_arm_hold_observer": (i32, [vp, P(i32), i32, i32, f64]),

@@ -93,7 +93,21 @@ struct rp_batch {
     double holdTolerance = 0.05;
     bool holdArmed = false;
 
+    // overlapped state copies (rp_batch_*_state_overlapped): device staging
+    // rows per readable array and for the kinematic input, the caller's copy
+    // stream, and the events that order the two streams
+    cudaStream_t copyStream = nullptr;
+    void* stageOut[3] = {nullptr, nullptr, nullptr};
+    void* stageIn = nullptr;
+    cudaEvent_t staged[3] = {nullptr, nullptr, nullptr};     // batch stream: rows staged
+    cudaEvent_t outCopied[3] = {nullptr, nullptr, nullptr};  // copy stream: staging read out
+    cudaEvent_t inReady = nullptr;                            // copy stream: input landed
+    cudaEvent_t inConsumed = nullptr;                         // batch stream: staging read
+
     ~rp_batch() {
+        for (cudaEvent_t e : {staged[0], staged[1], staged[2], outCopied[0], outCopied[1], outCopied[2], inReady,
+                              inConsumed})
+            if (e) cudaEventDestroy(e);
         if (graphExec) cudaGraphExecDestroy(graphExec);
         for (void* p : owned) cudaFree(p);
         if (ownStream && stream) cudaStreamDestroy(stream);

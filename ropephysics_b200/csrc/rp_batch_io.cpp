@@ -402,6 +402,82 @@ rp_status rp_batch_write_state_async(rp_batch* b, int32_t what, const void* src,
     return RP_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// The device array behind a readable RP_STATE_* and its size in bytes.
+bool readable(const rp_batch* b, int32_t what, const void** src, int64_t* size) {
+    switch (what) {
+        case RP_STATE_POSITIONS: *src = b->a.x; *size = b->totalP * 16; return true;
+        case RP_STATE_FRAMES: *src = b->a.q; *size = b->totalS * 16; return true;
+        case RP_STATE_CONTACTS: *src = b->a.contactState; *size = b->totalSlots; return true;
+        default: return false;
+    }
+}
+
+rp_status makeEvent(cudaEvent_t* e) {
+    if (!*e) RP_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    return RP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+rp_status rp_batch_set_copy_stream(rp_batch* b, void* stream) {
+    if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
+    rp_status st = syncBatch(b);
+    if (st != RP_OK) return st;
+    if (b->copyStream) RP_CUDA(cudaStreamSynchronize(b->copyStream));
+    b->copyStream = static_cast<cudaStream_t>(stream);
+    return RP_OK;
+}
+
+rp_status rp_batch_read_state_overlapped(rp_batch* b, int32_t what, void* dst, int64_t bytes) {
+    if (!b || !dst) return fail(RP_ERR_INVALID, "batch or dst is NULL");
+    if (!b->copyStream) return fail(RP_ERR_INVALID, "no copy stream: call rp_batch_set_copy_stream first");
+    const void* src = nullptr;
+    int64_t size = 0;
+    if (!readable(b, what, &src, &size)) return fail(RP_ERR_INVALID, "unknown state array for reading");
+    if (bytes != size) return fail(RP_ERR_INVALID, "bytes must be " + std::to_string(size));
+    if (size == 0) return RP_OK;
+    rp_status st;
+    if (!b->stageOut[what] && (st = b->alloc(reinterpret_cast<uint8_t*&>(b->stageOut[what]), size_t(size),
+                                             false)) != RP_OK)
+        return st;
+    if ((st = makeEvent(&b->staged[what])) != RP_OK || (st = makeEvent(&b->outCopied[what])) != RP_OK) return st;
+    // the previous read of this array has left the staging rows
+    RP_CUDA(cudaStreamWaitEvent(b->stream, b->outCopied[what], 0));
+    RP_CUDA(cudaMemcpyAsync(b->stageOut[what], src, size_t(size), cudaMemcpyDeviceToDevice, b->stream));
+    RP_CUDA(cudaEventRecord(b->staged[what], b->stream));
+    RP_CUDA(cudaStreamWaitEvent(b->copyStream, b->staged[what], 0));
+    RP_CUDA(cudaMemcpyAsync(dst, b->stageOut[what], size_t(size), cudaMemcpyDeviceToHost, b->copyStream));
+    RP_CUDA(cudaEventRecord(b->outCopied[what], b->copyStream));
+    return RP_OK;
+}
+
+rp_status rp_batch_write_state_overlapped(rp_batch* b, int32_t what, const void* src, int64_t bytes) {
+    if (!b || !src) return fail(RP_ERR_INVALID, "batch or src is NULL");
+    if (!b->copyStream) return fail(RP_ERR_INVALID, "no copy stream: call rp_batch_set_copy_stream first");
+    if (what != RP_STATE_KINEMATIC) return fail(RP_ERR_INVALID, "only RP_STATE_KINEMATIC is writable");
+    const int64_t size = b->totalP * 16;
+    if (bytes != size) return fail(RP_ERR_INVALID, "bytes must be " + std::to_string(size));
+    if (size == 0) return RP_OK;
+    rp_status st;
+    if (!b->stageIn && (st = b->alloc(reinterpret_cast<uint8_t*&>(b->stageIn), size_t(size), false)) != RP_OK)
+        return st;
+    if ((st = makeEvent(&b->inReady)) != RP_OK || (st = makeEvent(&b->inConsumed)) != RP_OK) return st;
+    // the previous write's rows have been taken from the staging buffer
+    RP_CUDA(cudaStreamWaitEvent(b->copyStream, b->inConsumed, 0));
+    RP_CUDA(cudaMemcpyAsync(b->stageIn, src, size_t(size), cudaMemcpyHostToDevice, b->copyStream));
+    RP_CUDA(cudaEventRecord(b->inReady, b->copyStream));
+    RP_CUDA(cudaStreamWaitEvent(b->stream, b->inReady, 0));
+    RP_CUDA(cudaMemcpyAsync(b->a.kinVel, b->stageIn, size_t(size), cudaMemcpyDeviceToDevice, b->stream));
+    RP_CUDA(cudaEventRecord(b->inConsumed, b->stream));
+    return RP_OK;
+}
+
 rp_status rp_batch_read_contact_states(rp_batch* b, uint8_t* out, int64_t cap, int64_t* count) {
     if (!b) return fail(RP_ERR_INVALID, "batch is NULL");
     if (count) *count = b->totalSlots;
