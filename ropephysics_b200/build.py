@@ -25,7 +25,10 @@ CXX = os.environ.get("CXX", "g++")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 INCLUDES = [f"-I{os.path.join(ROOT, 'include')}", f"-I{CSRC}", f"-I{os.path.join(CUDA_HOME, 'include')}"]
-NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"] + ARCH
+# --fmad=false: no multiply-add is fused unless the source says so (__fmaf_rn),
+# so every kernel rounds the reference-order arithmetic identically
+NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+              "--fmad=false"] + ARCH
 CXX_FLAGS = ["-std=c++17", "-O3", "-fPIC", "-Wall", "-Wextra", "-Wno-unused-parameter"]
 
 CU_SOURCES = ["rp_plain.cu", "rp_batched.cu", "rp_static_scratch.cu", "rp_traj.cu", "rp_harness.cu",

@@ -1,13 +1,27 @@
 // rp_math.cuh -- FP32 vector/quaternion/matrix algebra for the rod kernels.
 //
 // The formulas are those of the reference's shared math (src/core/math3.h and
-// src/core/geometry.h): the algorithm, and with it the order of every
-// floating-point operation, must be the same for the GPU results to agree
-// with the reference's FP32 GPU path to rounding. In particular
-// "vector / scalar" is "vector * (1 / scalar)" (math3.h:75-78), and
-// expression trees are kept in the reference's association so that nvcc's
-// FMA contraction makes the same choices. The code is written for this
-// library (register-friendly structs, no templates on the scalar).
+// src/core/geometry.h), and so is every floating-point operation and its
+// order, so that the results equal the reference's FP32 GPU kernel
+// (src/gpu/gpu_solver.cu) bit for bit. In particular "vector / scalar" is
+// "vector * (1 / scalar)" (math3.h:75-78).
+//
+// The reference is built with nvcc's default FMA contraction, and which
+// multiply-add pairs the compiler fuses is not fixed by the source: in
+// a * b + c * d either product can be the fused one, and the choice follows
+// the surrounding code. This library is therefore compiled with contraction
+// off (--fmad=false) and every fused multiply-add the reference's kernel
+// performs is written out with __fmaf_rn, so each kernel here -- batched,
+// one rod per CTA, state in global memory -- computes the same operations
+// whatever code surrounds them. The fused forms below are the ones the
+// reference's kernel was measured to produce (its outputs after single
+// substeps compared with every candidate rounding sequence, on rods with
+// generic frame orientations, loads, all primitive types and self-contacts):
+// in a * b + c * d and a * b - c * d the first product is fused, a chain of
+// sums fuses each further product into the running sum, and where a
+// conjugated quaternion or a skew matrix negates operands the fused product
+// is the other one (rotateInv, qmulConj, sandwichDiag of a skew matrix, and
+// the normalisation inside applyBodyDelta).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -30,14 +44,36 @@ __device__ __forceinline__ float4 f4(V3 a) { return make_float4(a.x, a.y, a.z, 0
 __device__ __forceinline__ Q4 q4(float4 a) { return Q4{a.x, a.y, a.z, a.w}; }
 __device__ __forceinline__ float4 f4(Q4 q) { return make_float4(q.w, q.x, q.y, q.z); }
 
+// one rounding each; with contraction off, plain * + - are these too
+__device__ __forceinline__ float fma3(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+// a * b + c * d and a * b - c * d, the first product fused
+__device__ __forceinline__ float pp(float a, float b, float c, float d) { return fma3(a, b, c * d); }
+__device__ __forceinline__ float pm(float a, float b, float c, float d) { return fma3(a, b, -(c * d)); }
+// the same with the second product fused
+__device__ __forceinline__ float ppB(float a, float b, float c, float d) { return fma3(c, d, a * b); }
+__device__ __forceinline__ float pmB(float a, float b, float c, float d) { return fma3(-c, d, a * b); }
+
 __device__ __forceinline__ V3 operator+(V3 a, V3 b) { return V3{a.x + b.x, a.y + b.y, a.z + b.z}; }
 __device__ __forceinline__ V3 operator-(V3 a, V3 b) { return V3{a.x - b.x, a.y - b.y, a.z - b.z}; }
 __device__ __forceinline__ V3 operator-(V3 a) { return V3{-a.x, -a.y, -a.z}; }
 __device__ __forceinline__ V3 operator*(V3 a, float s) { return V3{a.x * s, a.y * s, a.z * s}; }
 __device__ __forceinline__ V3 divs(V3 a, float s) { return a * (1.0f / s); }
-__device__ __forceinline__ float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+// c + a * s, fused per component
+__device__ __forceinline__ V3 fmav(V3 a, float s, V3 c) {
+    return V3{fma3(a.x, s, c.x), fma3(a.y, s, c.y), fma3(a.z, s, c.z)};
+}
+// c + cwise(a, b), fused per component
+__device__ __forceinline__ V3 fmacw(V3 a, V3 b, V3 c) {
+    return V3{fma3(a.x, b.x, c.x), fma3(a.y, b.y, c.y), fma3(a.z, b.z, c.z)};
+}
+// (ax bx + ay by) + az bz
+__device__ __forceinline__ float dot(V3 a, V3 b) { return fma3(a.z, b.z, pp(a.x, b.x, a.y, b.y)); }
+__device__ __forceinline__ float dotB(V3 a, V3 b) { return fma3(a.z, b.z, ppB(a.x, b.x, a.y, b.y)); }
 __device__ __forceinline__ V3 cross(V3 a, V3 b) {
-    return V3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+    return V3{pm(a.y, b.z, a.z, b.y), pm(a.z, b.x, a.x, b.z), pm(a.x, b.y, a.y, b.x)};
+}
+__device__ __forceinline__ V3 crossB(V3 a, V3 b) {
+    return V3{pmB(a.y, b.z, a.z, b.y), pmB(a.z, b.x, a.x, b.z), pmB(a.x, b.y, a.y, b.x)};
 }
 __device__ __forceinline__ float norm2(V3 a) { return dot(a, a); }
 __device__ __forceinline__ float norm(V3 a) { return sqrtf(dot(a, a)); }
@@ -82,15 +118,21 @@ __device__ __forceinline__ M3 mscale(const M3& A, float s) {
         for (int j = 0; j < 3; ++j) r.m[i][j] = A.m[i][j] * s;
     return r;
 }
-// A diag(d) A^T
+// A diag(d) A^T: (A_i0 d_x) A_j0 + (A_i1 d_y) A_j1 + (A_i2 d_z) A_j2. SKEW:
+// A is a skew matrix, whose negated entries make the second product the
+// fused one in the first sum.
+template <bool SKEW>
 __device__ __forceinline__ M3 sandwichDiag(const M3& A, V3 d) {
     M3 r;
 #pragma unroll
-    for (int i = 0; i < 3; ++i)
+    for (int i = 0; i < 3; ++i) {
+        const float p0 = A.m[i][0] * d.x, p1 = A.m[i][1] * d.y, p2 = A.m[i][2] * d.z;
 #pragma unroll
-        for (int j = 0; j < 3; ++j)
-            r.m[i][j] = A.m[i][0] * d.x * A.m[j][0] + A.m[i][1] * d.y * A.m[j][1] +
-                        A.m[i][2] * d.z * A.m[j][2];
+        for (int j = 0; j < 3; ++j) {
+            const float s = SKEW ? ppB(p0, A.m[j][0], p1, A.m[j][1]) : pp(p0, A.m[j][0], p1, A.m[j][1]);
+            r.m[i][j] = fma3(p2, A.m[j][2], s);
+        }
+    }
     return r;
 }
 // Symmetric positive-definite 3x3 solve by Cholesky; false if not SPD.
@@ -100,30 +142,38 @@ __device__ __forceinline__ bool solveSPD3(const M3& A, V3 b, V3& y) {
     l00 = sqrtf(l00);
     const float l10 = A.m[1][0] / l00;
     const float l20 = A.m[2][0] / l00;
-    float l11 = A.m[1][1] - l10 * l10;
+    float l11 = fma3(-l10, l10, A.m[1][1]);
     if (l11 <= 0.0f) return false;
     l11 = sqrtf(l11);
-    const float l21 = (A.m[2][1] - l20 * l10) / l11;
-    float l22 = A.m[2][2] - l20 * l20 - l21 * l21;
+    const float l21 = fma3(-l20, l10, A.m[2][1]) / l11;
+    float l22 = fma3(-l21, l21, fma3(-l20, l20, A.m[2][2]));
     if (l22 <= 0.0f) return false;
     l22 = sqrtf(l22);
     const float z0 = b.x / l00;
-    const float z1 = (b.y - l10 * z0) / l11;
-    const float z2 = (b.z - l20 * z0 - l21 * z1) / l22;
+    const float z1 = fma3(-l10, z0, b.y) / l11;
+    const float z2 = fma3(-l21, z1, fma3(-l20, z0, b.z)) / l22;
     y.z = z2 / l22;
-    y.y = (z1 - l21 * y.z) / l11;
-    y.x = (z0 - l10 * y.y - l20 * y.z) / l00;
+    y.y = fma3(-l21, y.z, z1) / l11;
+    y.x = fma3(-l20, y.z, fma3(-l10, y.y, z0)) / l00;
     return true;
 }
 
 __device__ __forceinline__ V3 im(Q4 q) { return V3{q.x, q.y, q.z}; }
 __device__ __forceinline__ Q4 qmake(float w, V3 v) { return Q4{w, v.x, v.y, v.z}; }
+__device__ __forceinline__ Q4 conj(Q4 q) { return Q4{q.w, -q.x, -q.y, -q.z}; }
 // Hamilton product: (aw bw - av.bv, aw bv + bw av + av x bv)
 __device__ __forceinline__ Q4 qmul(Q4 a, Q4 b) {
     const V3 av = im(a), bv = im(b);
-    return qmake(a.w * b.w - dot(av, bv), bv * a.w + av * b.w + cross(av, bv));
+    const V3 s{pp(bv.x, a.w, av.x, b.w), pp(bv.y, a.w, av.y, b.w), pp(bv.z, a.w, av.z, b.w)};
+    return qmake(fma3(a.w, b.w, -dot(av, bv)), s + cross(av, bv));
 }
-__device__ __forceinline__ Q4 conj(Q4 q) { return Q4{q.w, -q.x, -q.y, -q.z}; }
+// conj(a) * b: the conjugate's negated vector makes the dot product and the
+// cross product fuse their second products
+__device__ __forceinline__ Q4 qmulConj(Q4 a, Q4 b) {
+    const V3 av = im(conj(a)), bv = im(b);
+    const V3 s{pp(bv.x, a.w, av.x, b.w), pp(bv.y, a.w, av.y, b.w), pp(bv.z, a.w, av.z, b.w)};
+    return qmake(fma3(a.w, b.w, -dotB(av, bv)), s + crossB(av, bv));
+}
 __device__ __forceinline__ Q4 qadd(Q4 a, Q4 b) {
     return Q4{a.w + b.w, a.x + b.x, a.y + b.y, a.z + b.z};
 }
@@ -131,28 +181,45 @@ __device__ __forceinline__ Q4 qsub(Q4 a, Q4 b) {
     return Q4{a.w - b.w, a.x - b.x, a.y - b.y, a.z - b.z};
 }
 __device__ __forceinline__ Q4 qscale(Q4 q, float s) { return Q4{q.w * s, q.x * s, q.y * s, q.z * s}; }
+// c + q * s, fused per component
+__device__ __forceinline__ Q4 qfma(Q4 q, float s, Q4 c) {
+    return Q4{fma3(q.w, s, c.w), fma3(q.x, s, c.x), fma3(q.y, s, c.y), fma3(q.z, s, c.z)};
+}
+// ((aw bw + ax bx) + ay by) + az bz
 __device__ __forceinline__ float qdot(Q4 a, Q4 b) {
-    return a.w * b.w + a.x * b.x + a.y * b.y + a.z * b.z;
+    return fma3(a.z, b.z, fma3(a.y, b.y, pp(a.w, b.w, a.x, b.x)));
+}
+__device__ __forceinline__ float qdotB(Q4 a, Q4 b) {
+    return fma3(a.z, b.z, fma3(a.y, b.y, ppB(a.w, b.w, a.x, b.x)));
 }
 __device__ __forceinline__ Q4 qnormalize(Q4 q) {
     const float n = sqrtf(qdot(q, q));
     return qscale(q, 1.0f / n);
 }
-// body -> world
+// body -> world: v + t w + u x t, t = 2 u x v
 __device__ __forceinline__ V3 rotate(Q4 q, V3 v) {
     const V3 u = im(q);
     const V3 t = cross(u, v) * 2.0f;
-    return v + t * q.w + cross(u, t);
+    return fmav(t, q.w, v) + cross(u, t);
 }
-__device__ __forceinline__ V3 rotateInv(Q4 q, V3 v) { return rotate(conj(q), v); }
-// q <- normalize(q * (1, theta / 2)), theta a body-frame rotation vector
+// world -> body, rotate(conj(q), v): the negated axis fuses the second
+// product of both cross products
+__device__ __forceinline__ V3 rotateInv(Q4 q, V3 v) {
+    const V3 u = im(conj(q));
+    const V3 t = crossB(u, v) * 2.0f;
+    return fmav(t, q.w, v) + crossB(u, t);
+}
+// q <- normalize(q * (1, theta / 2)), theta a body-frame rotation vector;
+// the unit scalar of (1, theta / 2) multiplies nothing
 __device__ __forceinline__ Q4 applyBodyDelta(Q4 q, V3 theta) {
-    return qnormalize(qmul(q, qmake(1.0f, theta * 0.5f)));
+    const V3 av = im(q), bv = theta * 0.5f;
+    const Q4 p = qmake(q.w - dot(av, bv), fmav(bv, q.w, av) + cross(av, bv));
+    const float n = sqrtf(qdotB(p, p));
+    return qscale(p, 1.0f / n);
 }
-// Representative on the same hemisphere as the identity.
-__device__ __forceinline__ Q4 sameHemisphereId(Q4 q) {
-    return qdot(q, Q4{1.0f, 0.0f, 0.0f, 0.0f}) < 0.0f ? qscale(q, -1.0f) : q;
-}
+// Representative on the same hemisphere as the identity (the sign of w
+// decides; the reference's dot with the identity only adds zeros to it).
+__device__ __forceinline__ Q4 sameHemisphereId(Q4 q) { return q.w < 0.0f ? qscale(q, -1.0f) : q; }
 
 // ---------------------------------------------------------------- geometry
 
@@ -187,7 +254,7 @@ __device__ __forceinline__ float signedDistance(const PrimF& P, V3 p, V3& n) {
         const V3 ab = P.b - P.a;
         const float len2 = norm2(ab);
         const float t = len2 < 1e-30f ? 0.0f : clamp01(dot(p - P.a, ab) / len2);
-        const V3 axisPoint = P.a + (P.b - P.a) * t;
+        const V3 axisPoint = fmav(P.b - P.a, t, P.a);  // a + (b - a) t
         return distanceToSphereLike(axisPoint, P.radius, p, n);
     }
     // box
@@ -315,9 +382,9 @@ __device__ __forceinline__ void closestPointsBetweenSegments(V3 p1, V3 q1, V3 p2
         return;
     }
     const float b = dot(d1, d2);
-    const float denom = a * e - b * b;
-    s = denom > eps ? clamp01((b * f - c * e) / denom) : 0.0f;
-    t = (b * s + f) / e;
+    const float denom = pm(a, e, b, b);
+    s = denom > eps ? clamp01(pm(b, f, c, e) / denom) : 0.0f;
+    t = fma3(b, s, f) / e;
     if (t < 0.0f) {
         t = 0.0f;
         s = clamp01(-c / a);

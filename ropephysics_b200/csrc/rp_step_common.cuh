@@ -65,18 +65,20 @@ struct RodView {
     float contactMargin;
 };
 
-// Position update x[i] += d. In reference order this is a plain FP32 add. In
-// compensated mode (RP_PRECISION_COMPENSATED) x is a Kahan sum whose running
-// error lives in xComp (true position = x - xComp), and the xPrev array holds
-// the substep's displacement accumulator instead of the start position: a
-// small number carried at full relative precision, which is what friction and
-// velocity recovery need (position differences near 1 m lose everything below
-// ~6e-8 m in FP32).
+// Position update x[i] += a s. In reference order this is one fused
+// multiply-add per component, as the reference's kernel computes every
+// "x += vector * scalar". In compensated mode (RP_PRECISION_COMPENSATED) x is
+// a Kahan sum whose running error lives in xComp (true position = x - xComp),
+// and the xPrev array holds the substep's displacement accumulator instead of
+// the start position: a small number carried at full relative precision,
+// which is what friction and velocity recovery need (position differences
+// near 1 m lose everything below ~6e-8 m in FP32).
 template <bool COMP>
-__device__ __forceinline__ void addPos(const RodView& V, int i, V3 d) {
+__device__ __forceinline__ void addPos(const RodView& V, int i, V3 a, float s) {
     if (!COMP) {
-        V.x[i] = f4(v3(V.x[i]) + d);
+        V.x[i] = f4(fmav(a, s, v3(V.x[i])));
     } else {
+        const V3 d = a * s;
         const float4 xs = V.x[i];
         const float4 cs = V.xComp[i];
         const V3 y = d - v3(cs);
@@ -154,7 +156,7 @@ __device__ __forceinline__ void projectStretchAt(const RodView& V, int k, int i0
     const V3 C = u - V3{0.0f, 0.0f, 1.0f};
 
     const V3 alpha = v3(sc) * (invH2 * V.complianceScale);
-    M3 A = madd(midentity((w0 + w1) / (l * l)), sandwichDiag(mskew(u), iI));
+    M3 A = madd(midentity((w0 + w1) / (l * l)), sandwichDiag<true>(mskew(u), iI));
     A.m[0][0] += alpha.x;
     A.m[1][1] += alpha.y;
     A.m[2][2] += alpha.z;
@@ -163,12 +165,12 @@ __device__ __forceinline__ void projectStretchAt(const RodView& V, int k, int i0
     // constraint's only one of the substep and its multiplier starts at zero
     const V3 lam = V.lamS ? v3(V.lamS[k]) : V3{0.0f, 0.0f, 0.0f};
     V3 dL;
-    if (!solveSPD3(A, -(C + cwise(alpha, lam)), dL)) return;
+    if (!solveSPD3(A, -fmacw(alpha, lam, C), dL)) return;
     if (V.lamS) V.lamS[k] = f4(lam + dL);
 
     const V3 world = rotate(q, dL);
-    addPos<COMP>(V, i0, -(world * (w0 / l)));
-    addPos<COMP>(V, i1, world * (w1 / l));
+    addPos<COMP>(V, i0, -world, w0 / l);
+    addPos<COMP>(V, i1, world, w1 / l);
     if (norm2(iI) > 0.0f) {
         const V3 theta = cwise(iI, cross(dL, u));
         if (COMP)
@@ -194,33 +196,33 @@ __device__ __forceinline__ void projectBendAt(const RodView& V, int k, int a, in
     const float lbar = bc.w;
     const Q4 qa = q4(V.q[a]);
     const Q4 qb = q4(V.q[b]);
-    const Q4 p = sameHemisphereId(qmul(conj(qa), qb));
-    const V3 C = im(p) * (2.0f / lbar) - v3(V.g->bRestD[k]);
+    const Q4 p = sameHemisphereId(qmulConj(qa, qb));
+    const V3 C = fmav(im(p), 2.0f / lbar, -v3(V.g->bRestD[k]));
 
     const M3 skewPv = mskew(im(p));
     const M3 Ja = mscale(madd(midentity(-p.w), skewPv), 1.0f / lbar);
     const M3 Jb = mscale(madd(midentity(p.w), skewPv), 1.0f / lbar);
 
     const V3 alpha = v3(bc) * (invH2 * V.complianceScale);
-    M3 A = madd(sandwichDiag(Ja, iIa), sandwichDiag(Jb, iIb));
+    M3 A = madd(sandwichDiag<false>(Ja, iIa), sandwichDiag<false>(Jb, iIb));
     A.m[0][0] += alpha.x;
     A.m[1][1] += alpha.y;
     A.m[2][2] += alpha.z;
 
     const V3 lam = V.lamB ? v3(V.lamB[k]) : V3{0.0f, 0.0f, 0.0f};
     V3 dL;
-    if (!solveSPD3(A, -(C + cwise(alpha, lam)), dL)) return;
+    if (!solveSPD3(A, -fmacw(alpha, lam, C), dL)) return;
     if (V.lamB) V.lamB[k] = f4(lam + dL);
 
     if (norm2(iIa) > 0.0f) {
-        const V3 g = (dL * -p.w - cross(im(p), dL)) * (1.0f / lbar);
+        const V3 g = fmav(dL, -p.w, -cross(im(p), dL)) * (1.0f / lbar);
         if (COMP)
             rotateFrameComp(V, a, cwise(iIa, g) * 0.5f);
         else
             V.q[a] = f4(applyBodyDelta(qa, cwise(iIa, g)));
     }
     if (norm2(iIb) > 0.0f) {
-        const V3 g = (dL * p.w - cross(im(p), dL)) * (1.0f / lbar);
+        const V3 g = fmav(dL, p.w, -cross(im(p), dL)) * (1.0f / lbar);
         if (COMP)
             rotateFrameComp(V, b, cwise(iIb, g) * 0.5f);
         else
@@ -375,21 +377,21 @@ __device__ __forceinline__ void projectSlots(const RodView& V, int i, unsigned l
         const float clamped = c.lambdaN + dLambda > 0.0f ? c.lambdaN + dLambda : 0.0f;
         dLambda = clamped - c.lambdaN;
         c.lambdaN = clamped;
-        if (dLambda != 0.0f) addPos<COMP>(V, i, n * (w * dLambda));
+        if (dLambda != 0.0f) addPos<COMP>(V, i, n, w * dLambda);
 
         if (c.friction <= 0.0f || c.lambdaN <= 0.0f) {
             c.state = 1;
             continue;
         }
         const V3 dp = dispOf<COMP>(V, i);
-        const V3 tangential = dp - n * dot(dp, n);
+        const V3 tangential = fmav(-n, dot(dp, n), dp);  // dp - n (dp . n)
         const float slide = norm(tangential);
         if (slide < 1e-15f) {
             c.state = 2;
             continue;
         }
         if (!FP64) {
-            const float budget = c.friction * c.lambdaN * w - c.applied;
+            const float budget = fma3(c.friction * c.lambdaN, w, -c.applied);
             if (budget <= 0.0f) {
                 c.state = 3;
                 continue;
@@ -397,7 +399,7 @@ __device__ __forceinline__ void projectSlots(const RodView& V, int i, unsigned l
             const float capped = slide < budget ? slide : budget;
             c.state = slide <= budget ? 2 : 3;
             c.applied += capped;
-            addPos<COMP>(V, i, tangential * (-capped / slide));
+            addPos<COMP>(V, i, tangential, -capped / slide);
         } else {
             const double tx = tangential.x, ty = tangential.y, tz = tangential.z;
             const double slideD = sqrt(tx * tx + ty * ty + tz * tz);
@@ -410,7 +412,7 @@ __device__ __forceinline__ void projectSlots(const RodView& V, int i, unsigned l
             const double capped = slideD < budget ? slideD : budget;
             c.state = slideD <= budget ? 2 : 3;
             c.applied = float(double(c.applied) + capped);
-            addPos<COMP>(V, i, tangential * float(-capped / slideD));
+            addPos<COMP>(V, i, tangential, float(-capped / slideD));
         }
     }
 }
@@ -442,7 +444,7 @@ struct SegPair {
 static __device__ __noinline__ SegPair segmentPairNarrow(V3 a0, V3 a1, V3 b0, V3 b1, float twoR) {
     SegPair r;
     closestPointsBetweenSegments(a0, a1, b0, b1, r.u, r.w);
-    r.delta = (a0 + (a1 - a0) * r.u) - (b0 + (b1 - b0) * r.w);
+    r.delta = fmav(a1 - a0, r.u, a0) - fmav(b1 - b0, r.w, b0);
     r.dist = norm(r.delta);
     r.separation = r.dist - twoR;
     return r;
@@ -508,7 +510,8 @@ __device__ __forceinline__ void querySelfSegment(const RodView& V, const SelfScr
                         c.weight[2] = -(1.0f - w);
                         c.weight[3] = -w;
                         float dotSum = 0.0f;
-                        for (int m = 0; m < 4; ++m) dotSum += c.weight[m] * dot(v3(V.x[c.idx[m]]), n);
+                        for (int m = 0; m < 4; ++m)
+                            dotSum = fma3(c.weight[m], dot(v3(V.x[c.idx[m]]), n), dotSum);
                         c.offset = dotSum - separation;
                         c.friction = selfFriction * V.frictionScale;
                         c.lambdaN = 0.0f;
@@ -601,37 +604,37 @@ __device__ __forceinline__ int buildProjectionColors(const DSelf* pool, int live
 template <bool COMP>
 __device__ __forceinline__ void projectSelf(const RodView& V, DSelf& c) {
     float wEff = 0.0f;
-    for (int m = 0; m < 4; ++m) wEff += c.weight[m] * c.weight[m] * V.g->invMass[c.idx[m]];
+    for (int m = 0; m < 4; ++m) wEff = fma3(c.weight[m] * c.weight[m], V.g->invMass[c.idx[m]], wEff);
     if (wEff <= 0.0f) return;
     const V3 n{c.nx, c.ny, c.nz};
 
     float C = -c.offset;
-    for (int m = 0; m < 4; ++m) C += c.weight[m] * dot(v3(V.x[c.idx[m]]), n);
+    for (int m = 0; m < 4; ++m) C = fma3(c.weight[m], dot(v3(V.x[c.idx[m]]), n), C);
     float dLambda = -C / wEff;
     const float clamped = c.lambdaN + dLambda > 0.0f ? c.lambdaN + dLambda : 0.0f;
     dLambda = clamped - c.lambdaN;
     c.lambdaN = clamped;
     if (dLambda != 0.0f)
         for (int m = 0; m < 4; ++m)
-            addPos<COMP>(V, c.idx[m], n * (V.g->invMass[c.idx[m]] * c.weight[m] * dLambda));
+            addPos<COMP>(V, c.idx[m], n, V.g->invMass[c.idx[m]] * c.weight[m] * dLambda);
 
     if (c.friction <= 0.0f || c.lambdaN <= 0.0f) return;
 
     V3 dp{0.0f, 0.0f, 0.0f};
     for (int m = 0; m < 4; ++m) {
         const int pi = c.idx[m];
-        dp = dp + dispOf<COMP>(V, pi) * c.weight[m];
+        dp = fmav(dispOf<COMP>(V, pi), c.weight[m], dp);
     }
-    const V3 tangential = dp - n * dot(dp, n);
+    const V3 tangential = fmav(-n, dot(dp, n), dp);  // dp - n (dp . n)
     const float slide = norm(tangential);
     if (slide < 1e-15f) return;
-    const float budget = c.friction * c.lambdaN * wEff - c.applied;
+    const float budget = fma3(c.friction * c.lambdaN, wEff, -c.applied);
     if (budget <= 0.0f) return;
     const float capped = slide < budget ? slide : budget;
     c.applied += capped;
     const V3 correction = tangential * (-capped / slide);
     for (int m = 0; m < 4; ++m)
-        addPos<COMP>(V, c.idx[m], correction * (V.g->invMass[c.idx[m]] * c.weight[m] / wEff));
+        addPos<COMP>(V, c.idx[m], correction, V.g->invMass[c.idx[m]] * c.weight[m] / wEff);
 }
 
 // ---------------------------------------------------------------- predict / finish
@@ -641,12 +644,12 @@ __device__ __forceinline__ void predictParticle(const RodView& V, int i, float h
     V.xPrev[i] = COMP ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : V.x[i];
     const float w = V.g->invMass[i];
     if (w == 0.0f) {
-        addPos<COMP>(V, i, v3(V.g->kin[i]) * h);  // prescribed motion
+        addPos<COMP>(V, i, v3(V.g->kin[i]), h);  // prescribed motion
         return;
     }
-    const V3 vn = v3(V.v[i]) + (g + v3(V.g->force[i]) * w) * h;
+    const V3 vn = fmav(fmav(v3(V.g->force[i]), w, g), h, v3(V.v[i]));  // v + (g + f w) h
     V.v[i] = f4(vn);
-    addPos<COMP>(V, i, vn * h);
+    addPos<COMP>(V, i, vn, h);
 }
 
 template <bool COMP>
@@ -660,12 +663,12 @@ __device__ __forceinline__ void predictFrame(const RodView& V, int j, float h) {
     const V3 w = v3(V.omega[j]);
     const Q4 q = q4(V.q[j]);
     const V3 tau = rotateInv(q, v3(V.g->torque[j]));
-    const V3 wn = w + cwise(iI, tau - cross(w, cwise(v3(V.g->inertia[j]), w))) * h;
+    const V3 wn = fmav(cwise(iI, tau - cross(w, cwise(v3(V.g->inertia[j]), w))), h, w);
     V.omega[j] = f4(wn);
     if (COMP)
         rotateFrameComp(V, j, wn * (0.5f * h));
     else
-        V.q[j] = f4(qnormalize(qadd(q, qscale(qmul(q, qmake(0.0f, wn)), 0.5f * h))));
+        V.q[j] = f4(qnormalize(qfma(qmul(q, qmake(0.0f, wn)), 0.5f * h, q)));
 }
 
 template <bool COMP>
@@ -689,7 +692,7 @@ __device__ __forceinline__ void finishFrame(const RodView& V, int j, float h, fl
         const Q4 e = q4(V.qPrev[j]);  // the substep's rotation 1 + e
         dq = sameHemisphereId(Q4{1.0f + e.w, e.x, e.y, e.z});
     } else {
-        dq = sameHemisphereId(qmul(conj(q4(V.qPrev[j])), q4(V.q[j])));
+        dq = sameHemisphereId(qmulConj(q4(V.qPrev[j]), q4(V.q[j])));
     }
     V.omega[j] = f4(im(dq) * (2.0f / h) * angDecay);
 }

@@ -22,7 +22,8 @@ printed, not asserted tightly.
             steps
   config 3  24 rods sampled from the uneven batch, each with its own world
             (1-4 primitives, self-collision), each in its own reference batch;
-            restarts after 0, 100 and 500 steps, and at every restart point
+            restarts after 0, 20, 100 and 500 steps (rods the reference runs
+            on its multi-kernel path: 0 and 20), and at every restart point
             the self-contact pair lists and world-contact active sets of one
             substep bit-exact against the reference kernel
 """
@@ -216,44 +217,36 @@ def _one_substep(p):
                          gravity=p.gravity)
 
 
-def test_uneven_sample_restarts_vs_reference_gpu(reference_gpu):
-    R = reference_gpu
-    _need(R)
-    draws = synth.uneven(16384, 0)
-    idx = np.random.default_rng(7).choice(len(draws), size=24, replace=False)
-    mat = dict(youngs=synth.YOUNGS, poisson=synth.POISSON, density=synth.DENSITY, radius=synth.RADIUS)
-    p = rp.StepParams(dt=1.0 / 60, substeps=50, iterations=1)
+# Restart points of the uneven sample: the rods start 2 cm clear of their
+# primitives and fall onto them within the first 20 steps. Rods the
+# reference runs fused (its 48 KB shared-memory budget) take every restart;
+# longer rods run on its multi-kernel path, whose self-collision is one
+# thread per rod (about 0.4 s per step for 500 segments), and take the first
+# two.
+UNEVEN_RESTARTS_FUSED = (0, 20, 100, 500)
+UNEVEN_RESTARTS_MULTI = (0, 20)
+
+
+def _uneven_restarts(R, refs, protos, worlds, owlds, p, restarts):
+    """Restart windows for one group of rods (each in its own reference
+    batch): at each restart the reference's state goes into this library,
+    one substep's pair lists and active sets are compared bit for bit, then
+    both step WINDOW steps. Returns the worst dx (relative to each rod's
+    length) and dq per restart, per rod, and the contacts compared."""
     one = _one_substep(p)
     g, g1 = _gravity(p), _gravity(one)
-    refs, protos, worlds, owlds = [], [], [], []
-    for i in idx:
-        d = draws[i]
-        h = R.centerline(d.points, frame_seed=(0.0, 0.0, 1.0), **mat)
-        rr = R.export(h)
-        rr.bRestD[:] = 0.0
-        R.import_state(h, rr)
-        ow = OW([OP(*q) for q in d.prims], True, d.friction, 2, d.hash_table_size, 0.25)
-        wh = R.world(ow)
-        rb = R.lib.refgpu_create(h, 1, 1, wh) or R.lib.refgpu_create(h, 1, 0, wh)  # fused if it fits
-        assert rb
-        refs.append((h, wh, rb, rr.nP, rr.nS, 0.2 * d.segments / 32))
-        protos.append(product_rod(rr))
-        owlds.append(ow)
-        worlds.append(rp.World([W.primitive(q) for q in d.prims], self_collision=True, self_friction=d.friction,
-                               hash_table_size=d.hash_table_size))
-    n = len(idx)
+    n = len(refs)
     rest = rp.Batch.create_mixed(protos, worlds, list(range(n)), rp.Strategy.BATCHED)
-    worst, pairs_total, active_total = {}, 0, 0
+    worst = {k: [[0.0, 0.0] for _ in range(n)] for k in restarts}
+    pairs_total = active_total = 0
     s = 0
-    for start in RESTARTS:
+    for start in restarts:
         for h, wh, rb, *_ in refs:
             R.lib.refgpu_step(rb, p.dt, p.substeps, p.iterations, g, 0.0, 0.0, 1, start - s)
         s = start
-        states = []
         for r, (h, wh, rb, nP, nS, _) in enumerate(refs):
             R.lib.refgpu_sync(rb)
             x, v, q, w = R.gpu_state(rb, 1, nP, nS)
-            states.append((x[0], v[0], q[0], w[0]))
             _load_state(rest, r, protos[r], x[0], v[0], q[0], w[0])
             # one substep from this state: pair lists and active sets exact
             # against the reference's multi-kernel path (its global pool)
@@ -285,23 +278,64 @@ def test_uneven_sample_restarts_vs_reference_gpu(reference_gpu):
                 R.lib.refgpu_step(rb, p.dt, p.substeps, p.iterations, g, 0.0, 0.0, 1, 1)
                 R.lib.refgpu_sync(rb)
                 rx, _, rq, _ = R.gpu_state(rb, 1, nP, nS)
-                dx = max_dx(rest.positions_of(r, xs), rx[0]) / length
-                dq = max_dq(rest.frames_of(r, qs), rq[0])
-                a = worst.setdefault(start, [0.0, 0.0])
-                a[0], a[1] = max(a[0], dx), max(a[1], dq)
+                a = worst[start][r]
+                a[0] = max(a[0], max_dx(rest.positions_of(r, xs), rx[0]) / length)
+                a[1] = max(a[1], max_dq(rest.frames_of(r, qs), rq[0]))
         s = start + WINDOW
-    print(f"\nuneven sample of {n} rods vs the reference GPU kernel: restart windows (max over {WINDOW} steps, "
-          "dx relative to the rod length) "
-          + ", ".join(f"after {k}: dx {v[0]:.2e} dq {v[1]:.2e}" for k, v in worst.items())
-          + f"; {pairs_total} self-contact pairs and {active_total} active world contacts bit-exact")
-    for k, (dx, dq) in worst.items():
-        assert dx <= TOL and dq <= TOL, (k, dx, dq)
-    assert pairs_total > 0 and active_total > 0
     assert rest.error_count() == 0
     rest.close()
-    for h, wh, rb, *_ in refs:
-        R.lib.refgpu_free(rb)
-        R.free(h)
+    return worst, pairs_total, active_total
+
+
+def test_uneven_sample_restarts_vs_reference_gpu(reference_gpu):
+    R = reference_gpu
+    _need(R)
+    draws = synth.uneven(16384, 0)
+    idx = np.random.default_rng(7).choice(len(draws), size=24, replace=False)
+    mat = dict(youngs=synth.YOUNGS, poisson=synth.POISSON, density=synth.DENSITY, radius=synth.RADIUS)
+    p = rp.StepParams(dt=1.0 / 60, substeps=50, iterations=1)
+    groups = {"fused": ([], [], [], []), "multi-kernel": ([], [], [], [])}
+    for i in idx:
+        d = draws[i]
+        h = R.centerline(d.points, frame_seed=(0.0, 0.0, 1.0), **mat)
+        rr = R.export(h)
+        rr.bRestD[:] = 0.0
+        R.import_state(h, rr)
+        ow = OW([OP(*q) for q in d.prims], True, d.friction, 2, d.hash_table_size, 0.25)
+        wh = R.world(ow)
+        rb = R.lib.refgpu_create(h, 1, 1, wh)
+        kind = "fused"
+        if not rb:
+            rb, kind = R.lib.refgpu_create(h, 1, 0, wh), "multi-kernel"
+        assert rb
+        refs, protos, worlds, owlds = groups[kind]
+        refs.append((h, wh, rb, rr.nP, rr.nS, 0.2 * d.segments / 32))
+        protos.append(product_rod(rr))
+        owlds.append(ow)
+        worlds.append(rp.World([W.primitive(q) for q in d.prims], self_collision=True, self_friction=d.friction,
+                               hash_table_size=d.hash_table_size))
+    results, pairs_total, active_total = {}, 0, 0
+    for kind, restarts in (("fused", UNEVEN_RESTARTS_FUSED), ("multi-kernel", UNEVEN_RESTARTS_MULTI)):
+        refs, protos, worlds, owlds = groups[kind]
+        if not refs:
+            continue
+        worst, pt, at = _uneven_restarts(R, refs, protos, worlds, owlds, p, restarts)
+        results[kind] = worst
+        pairs_total += pt
+        active_total += at
+        for k, rows in worst.items():
+            print(f"\nuneven sample, {kind} path ({len(refs)} rods), restart after {k} (max over {WINDOW} "
+                  "steps, dx relative to the rod length): "
+                  + " ".join(f"{refs[r][3] - 1}:{dx:.1e}/{dq:.1e}" for r, (dx, dq) in enumerate(rows)))
+        for h, wh, rb, *_ in refs:
+            R.lib.refgpu_free(rb)
+            R.free(h)
+    print(f"\nuneven sample: {pairs_total} self-contact pairs and {active_total} active world contacts bit-exact")
+    for kind, worst in results.items():
+        for k, rows in worst.items():
+            for r, (dx, dq) in enumerate(rows):
+                assert dx <= TOL and dq <= TOL, (kind, k, r, dx, dq)
+    assert pairs_total > 0 and active_total > 0
 
 
 # ----------------------------------------------------------------------------- error vs FP64

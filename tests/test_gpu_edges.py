@@ -87,18 +87,32 @@ def test_sixty_four_primitives():
 
 
 def test_refused_precision_change_keeps_the_plan(oracle64):
-    """A clamped rod of 1700 segments fits the batched kernel's shared memory
-    in reference precision (lean layout 128 n + 416 bytes = 218 KB) but not
-    compensated (144 n + 432 bytes = 245 KB > 227 KB). Switching it to
-    compensated precision must fail with RP_ERR_SHARED_MEMORY and leave the
-    batch's plan as it was: same shared memory per CTA, and steps bitwise
-    equal to a batch that never tried."""
-    n = 1700
-    o = oracle64.straight(n, 1.7, youngs=1e8, poisson=0.3, density=1100.0, radius=5e-3)
-    oracle64.clamp(o, False)
-    proto = product_rod(o)
-    b = rp.Batch.create(proto, 2, rp.Strategy.BATCHED)
-    smem = b.shared_bytes_per_block
+    """A clamped rod long enough to fit the batched kernel's shared memory in
+    reference precision but not compensated (its layout adds the Kahan
+    compensation rows of positions and frames): switching it to compensated
+    precision must fail with RP_ERR_SHARED_MEMORY and leave the batch's plan
+    as it was -- same shared memory per CTA, and steps bitwise equal to a
+    batch that never tried. The length is the first of a ladder that splits
+    the two layouts on this device."""
+    proto = b = smem = None
+    for n in range(1500, 3001, 100):
+        o = oracle64.straight(n, n / 1000.0, youngs=1e8, poisson=0.3, density=1100.0, radius=5e-3)
+        oracle64.clamp(o, False)
+        cand = product_rod(o)
+        try:
+            trial = rp.Batch.create(cand, 2, rp.Strategy.BATCHED)
+        except rp.RopeError:
+            break  # too long even for reference precision
+        smem = trial.shared_bytes_per_block
+        try:
+            trial.set_precision(int(rp.Precision.COMPENSATED))
+        except rp.RopeError as e:
+            assert e.status == 3 and "shared memory" in str(e)
+            proto, b = cand, trial
+            break
+        trial.close()
+    assert b is not None, "no rod length splits the reference and compensated layouts"
+    assert b.shared_bytes_per_block == smem
     with pytest.raises(rp.RopeError) as e:
         b.set_precision(int(rp.Precision.COMPENSATED))
     assert e.value.status == 3 and "shared memory" in str(e.value)

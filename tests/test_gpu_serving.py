@@ -86,21 +86,25 @@ def test_budget_admission_and_queueing():
         sizes.append(probe.info(rid)["resident_bytes"])
     probe.drain(300)
     probe.close()
-    # the smallest budget, in steps of 1/8, whose arenas take the largest
-    # request: every request fits alone, and the six cannot all be resident
-    # at once, so later ones wait for earlier ones to retire
-    big = reqs[int(np.argmax(sizes))]
+    # the smallest budget, in steps of 1/8, whose arenas take every request
+    # alone (the arenas split the budget in fixed proportions, so the request
+    # that binds may be one with many contact slots rather than the largest):
+    # the six cannot all be resident at once, so later ones wait for earlier
+    # ones to retire
     budget = max(max(sizes), 1 << 20)
     for _ in range(64):
-        probe = rp.Server(budget, PARAMS)
-        try:
-            submit(probe, big)
-            fits = True
-        except rp.RopeError as e:
-            assert e.status == 6
-            fits = False
-        probe.drain(300)
-        probe.close()
+        fits = True
+        for r in reqs:
+            probe = rp.Server(budget, PARAMS)
+            try:
+                submit(probe, r)
+            except rp.RopeError as e:
+                assert e.status == 6
+                fits = False
+            probe.drain(300)
+            probe.close()
+            if not fits:
+                break
         if fits:
             break
         budget = int(budget * 1.125)
