@@ -43,7 +43,7 @@ sys.path.insert(0, ROOT)
 #               window the shape timing measures), bar, floor, self-collision
 #   grid        a pinned 64-segment rod over the floor plane
 #   cantilever  a pinned 64-segment rod, no contacts
-FLOPS_PER_SEG_SUBSTEP = {"uneven": 1696.2, "hook": 1463.8, "grid": 890.5, "cantilever": 880.5}
+FLOPS_PER_SEG_SUBSTEP = {"uneven": 1696.2, "hook": 1446.1, "grid": 890.5, "cantilever": 880.5}
 # Algorithmic HBM bytes per segment per step: state read once and written once
 # (x, v, force, kinematic velocity per particle; q, omega, torque per frame;
 # float4 rows): read 4 x 16 + 3 x 16, written 2 x 16 + 2 x 16.

@@ -196,7 +196,7 @@ static rp_status createImpl(const rp_rod_desc* const* rods, int numRods, const r
         }
         R.slotOff = b->totalSlots;
         R.poolOff = int(b->totalPool);
-        R.hashOff = int(b->totalHash);
+        R.hashOff = b->totalHash;
         b->totalP += T.nP;
         b->totalS += T.nS;
         b->totalSt += T.nSt;

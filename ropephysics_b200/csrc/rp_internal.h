@@ -49,7 +49,7 @@ struct DRod {
     int64_t slotOff;               // contact slot offset: pOff * maxPrims
     int32_t selfCollision, selfGap, selfCapacity, hashTableSize;
     int32_t poolOff;               // self-contact pool offset (selfCapacity entries)
-    int32_t hashOff;               // self-contact scratch offset into gHash: the plain
+    int64_t hashOff;               // self-contact scratch offset into gHash: the plain
                                    // kernel's hash (hashTableSize + 1 ints); the batched
                                    // kernel's hash, cursors and levels
                                    // (2 (hashTableSize + 1) + 3 (selfCapacity + 1) ints)
@@ -164,7 +164,7 @@ struct DArgs {
     float4* gCentres;  // per segment
     int32_t* gSelfInt; // per segment: plain kernel 4 ints (cellOf, sorted, count,
                        // start) at 4 stOff; batched 2 ints (cellOf, sorted) at 2 stOff
-    int32_t* gHash;    // per rod at hashOff (see DRod::hashOff)
+    int32_t* gHash;    // per rod at hashOff (see DRod::hashOff; 64-bit: the largest arena)
     DSelf* gPool;      // selfCapacity per rod
     int32_t* gMisc;    // 4 per rod: cell size (float bits), live, overflow, pad
 

@@ -254,7 +254,7 @@ bool rp_server::admit(Request& rq) {
         R.primOff += int32_t(o[PRIM]);
         R.slotOff += o[SLOT];
         R.poolOff += int32_t(o[POOL]);
-        R.hashOff += int32_t(o[HASH]);
+        R.hashOff += o[HASH];
         rq.rodIds[i] = int32_t(o[ROD]) + i;
         hRods[size_t(o[ROD]) + i] = R;
     }
@@ -506,8 +506,8 @@ rp_status rp_server_create(const rp_server_config* cfg, rp_server** out) {
     const int64_t probeP = int64_t(1) << 20;
     const int64_t P = std::max<int64_t>(int64_t(double(probeP) * double(B) / double(capacities(probeP))), 4096);
     const int64_t arenaBytes = capacities(P);
-    for (int u = 0; u < NUNITS; ++u)
-        if (cap[u] > int64_t(INT32_MAX)) {
+    for (int u = 0; u < NUNITS; ++u)  // every offset is 32-bit but the hash arena's
+        if (u != HASH && cap[u] > int64_t(INT32_MAX)) {
             delete s;
             return fail(RP_ERR_INVALID, "budget too large: device offsets are 32-bit");
         }
@@ -680,7 +680,7 @@ rp_status rp_server_submit(rp_server* s, const rp_request* r, uint64_t* id) {
         }
         R.slotOff = Q.counts[SLOT];
         R.poolOff = int32_t(Q.counts[POOL]);
-        R.hashOff = int32_t(Q.counts[HASH]);
+        R.hashOff = Q.counts[HASH];
         Q.rods.push_back(R);
         const size_t p0 = Q.x.size(), s0 = Q.q.size();
         Q.x.resize(p0 + T.nP);

@@ -200,6 +200,10 @@ def hanging_cable_points(leg_ratio: float, length=1.2, segments=120, bar_radius=
 
 
 HOOK_MATERIAL = dict(poisson=0.35, density=1100.0, radius=0.004)
+# The floor of the hook sweep, below the lowest point of every drape: a
+# 1.2 m cable over the bar at 0.8 m reaches 0.1 m below z = 0 at the 4:1
+# ratio, so a floor at 0 would start those placements inside it.
+HOOK_FLOOR_Z = -0.25
 
 
 def hook(ratios: int = 60, frictions: int = 30, stiffnesses=(1e8, 3e8)) -> Workload:
@@ -210,7 +214,7 @@ def hook(ratios: int = 60, frictions: int = 30, stiffnesses=(1e8, 3e8)) -> Workl
     for E in stiffnesses:
         for mu in mus:
             w = World([Primitive.capsule((0.0, -0.3, 0.8), (0.0, 0.3, 0.8), 0.02, float(mu)),
-                       Primitive.plane((0.0, 0.0, 0.0), (0.0, 0.0, 1.0), float(mu))],
+                       Primitive.plane((0.0, 0.0, HOOK_FLOOR_Z), (0.0, 0.0, 1.0), float(mu))],
                       self_collision=True, self_friction=float(mu), hash_table_size=256)
             worlds.append(w)
             for r in rs:

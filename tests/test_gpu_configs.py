@@ -494,9 +494,9 @@ def test_error_vs_fp64_hook(reference_gpu, oracle64):
         orods.append(o)
         protos.append(product_rod(o))
         oworlds.append(OW([OP.capsule((0.0, -0.3, 0.8), (0.0, 0.3, 0.8), 0.02, mu),
-                           OP.plane((0, 0, 0), (0, 0, 1), mu)], True, mu, 2, 256, 0.25))
+                           OP.plane((0, 0, W.HOOK_FLOOR_Z), (0, 0, 1), mu)], True, mu, 2, 256, 0.25))
         worlds.append(rp.World([rp.Primitive.capsule((0.0, -0.3, 0.8), (0.0, 0.3, 0.8), 0.02, mu),
-                                rp.Primitive.plane((0, 0, 0), (0, 0, 1), mu)],
+                                rp.Primitive.plane((0, 0, W.HOOK_FLOOR_Z), (0, 0, 1), mu)],
                                self_collision=True, self_friction=mu, hash_table_size=256))
     rows = _run_three(R, orods, oworlds, oparams(p), protos, worlds, p, (1, 10, 100, 480))
     _print_rows("hook", rows)

@@ -80,13 +80,13 @@ def harness_style_verdicts(ratios, mus, youngs, p):
         handles = [R.hanging(float(ratios[n]), float(E), length=1.2, segments=120, bar_radius=0.02,
                              bar_height=0.8) for n in members]
         ow = OW([OP.capsule((0, -0.3, 0.8), (0, 0.3, 0.8), 0.02, float(mu)),
-                 OP.plane((0, 0, 0), (0, 0, 1), float(mu))],
+                 OP.plane((0, 0, W.HOOK_FLOOR_Z), (0, 0, 1), float(mu))],
                 self_collision=True, self_friction=float(mu), hash_table_size=256)
         rb = R.lib.refgpu_create(handles[0], len(members), 1, R.world(ow))
         assert rb
         cables = [product_rod(R.export(h)) for h in handles]
         world = rp.World([rp.Primitive.capsule((0, -0.3, 0.8), (0, 0.3, 0.8), 0.02, float(mu)),
-                          rp.Primitive.plane((0, 0, 0), (0, 0, 1), float(mu))],
+                          rp.Primitive.plane((0, 0, W.HOOK_FLOOR_Z), (0, 0, 1), float(mu))],
                          self_collision=True, self_friction=float(mu), hash_table_size=256)
         b = rp.Batch.create(cables[0], len(members), rp.Strategy.BATCHED, world)
         z0 = []
@@ -141,7 +141,7 @@ def test_hook_sweep_verdicts_vs_fp64_cpu(reference):
         # the reference's drape builder (straight rest shape) at the sweep's
         # geometry; the product builds the same doubles (host tests)
         worlds.append(reference.world(OW([OP.capsule((0, -0.3, 0.8), (0, 0.3, 0.8), 0.02, mu),
-                                          OP.plane((0, 0, 0), (0, 0, 1), mu)],
+                                          OP.plane((0, 0, W.HOOK_FLOOR_Z), (0, 0, 1), mu)],
                                          self_collision=True, self_friction=mu, hash_table_size=256)))
     p = Params(dt=float(np.float32(1.0 / 60)), substeps=20, iterations=1,
                gravity=(0.0, 0.0, float(np.float32(-9.81))))

@@ -292,7 +292,7 @@ def test_flops_per_segment_substep_hook_sweep():
         r = oc.centerline(W.hanging_cable_points(ratio), youngs=youngs, frame_seed=(0, 1, 0),
                           **W.HOOK_MATERIAL)
         r.bRestD[:] = 0.0
-        w = OW([OP.capsule((0.0, -0.3, 0.8), (0.0, 0.3, 0.8), 0.02, mu), OP.plane((0, 0, 0), (0, 0, 1), mu)],
+        w = OW([OP.capsule((0.0, -0.3, 0.8), (0.0, 0.3, 0.8), 0.02, mu), OP.plane((0, 0, W.HOOK_FLOOR_Z), (0, 0, 1), mu)],
                True, mu, 2, 256, 0.25)
         rods.append((r, w, Context(dtype=np.float64), 120))
     assert _counted_window(oc, rods, p, 23, 20) == pytest.approx(bench.FLOPS_PER_SEG_SUBSTEP["hook"], abs=0.05)
