@@ -149,8 +149,12 @@ rp_status rp_batch_autotune(rp_batch* b, const rp_step_params* p, int32_t max_st
         }
     }
     // one rod per CTA (the plain kernel), when every rod's full layout fits:
-    // it wins for a few short rods, where the batched teams leave lanes idle
-    if (st == RP_OK && bestMs < 3.0e38f && reservePlain(b) == RP_OK) {
+    // it wins for a few short rods, where the batched teams leave lanes idle;
+    // beyond one rod per SM the batched packing wins, and the trial launches
+    // of a large batch would cost seconds
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+    if (st == RP_OK && bestMs < 3.0e38f && b->numRods <= sms && reservePlain(b) == RP_OK) {
         b->tune.plain = true;
         float ms = 0.0f;
         st = snap.restore(b);
