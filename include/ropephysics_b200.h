@@ -430,12 +430,15 @@ rp_status rp_batch_write_state_async(rp_batch* batch, int32_t what, const void* 
  * cudaStream_t) while later steps run on the batch's stream. A read first
  * copies the rows on the device into a staging buffer the batch owns (after
  * the work queued so far on the batch's stream, a few tens of microseconds),
- * then to `dst` on the copy stream; a write lands in a staging buffer on the
- * copy stream and is moved into place on the batch's stream before the next
- * step. Host buffers must stay valid until the copy stream has passed the
- * copy (record and wait an event on it); reading the same array again, or
- * writing again, waits on the device for the previous copy out of (into) the
- * staging buffer. The first call per array allocates its staging buffer. */
+ * then to `dst` on the copy stream; a write crosses on an input stream the
+ * batch owns (on the copy stream it would queue behind the previous step's
+ * reads, which wait for that step) into a staging buffer and is moved into
+ * place on the batch's stream before the next step. A read's host buffer
+ * must stay valid until the copy stream has passed the copy (record and wait
+ * an event on it), a write's until the batch's stream has passed the next
+ * step; reading the same array again, or writing again, waits on the device
+ * for the previous copy out of (into) the staging buffer. The first call per
+ * array allocates its staging buffer. */
 rp_status rp_batch_set_copy_stream(rp_batch* batch, void* cuda_stream);
 rp_status rp_batch_read_state_overlapped(rp_batch* batch, int32_t what, void* dst, int64_t bytes);
 rp_status rp_batch_write_state_overlapped(rp_batch* batch, int32_t what, const void* src, int64_t bytes);

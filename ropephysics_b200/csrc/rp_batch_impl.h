@@ -95,8 +95,12 @@ struct rp_batch {
 
     // overlapped state copies (rp_batch_*_state_overlapped): device staging
     // rows per readable array and for the kinematic input, the caller's copy
-    // stream, and the events that order the two streams
+    // stream (outputs), the batch's own input stream (inputs: on the copy
+    // stream they would queue behind the previous step's outputs, which wait
+    // for that step, and the next step would wait for them), and the events
+    // that order the streams
     cudaStream_t copyStream = nullptr;
+    cudaStream_t inStream = nullptr;
     void* stageOut[3] = {nullptr, nullptr, nullptr};
     void* stageIn = nullptr;
     cudaEvent_t staged[3] = {nullptr, nullptr, nullptr};     // batch stream: rows staged
@@ -111,6 +115,7 @@ struct rp_batch {
         if (graphExec) cudaGraphExecDestroy(graphExec);
         for (void* p : owned) cudaFree(p);
         if (ownStream && stream) cudaStreamDestroy(stream);
+        if (inStream) cudaStreamDestroy(inStream);
     }
 
     template <typename T>

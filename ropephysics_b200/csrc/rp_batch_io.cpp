@@ -468,10 +468,11 @@ rp_status rp_batch_write_state_overlapped(rp_batch* b, int32_t what, const void*
     if (!b->stageIn && (st = b->alloc(reinterpret_cast<uint8_t*&>(b->stageIn), size_t(size), false)) != RP_OK)
         return st;
     if ((st = makeEvent(&b->inReady)) != RP_OK || (st = makeEvent(&b->inConsumed)) != RP_OK) return st;
+    if (!b->inStream) RP_CUDA(cudaStreamCreateWithFlags(&b->inStream, cudaStreamNonBlocking));
     // the previous write's rows have been taken from the staging buffer
-    RP_CUDA(cudaStreamWaitEvent(b->copyStream, b->inConsumed, 0));
-    RP_CUDA(cudaMemcpyAsync(b->stageIn, src, size_t(size), cudaMemcpyHostToDevice, b->copyStream));
-    RP_CUDA(cudaEventRecord(b->inReady, b->copyStream));
+    RP_CUDA(cudaStreamWaitEvent(b->inStream, b->inConsumed, 0));
+    RP_CUDA(cudaMemcpyAsync(b->stageIn, src, size_t(size), cudaMemcpyHostToDevice, b->inStream));
+    RP_CUDA(cudaEventRecord(b->inReady, b->inStream));
     RP_CUDA(cudaStreamWaitEvent(b->stream, b->inReady, 0));
     RP_CUDA(cudaMemcpyAsync(b->a.kinVel, b->stageIn, size_t(size), cudaMemcpyDeviceToDevice, b->stream));
     RP_CUDA(cudaEventRecord(b->inConsumed, b->stream));
