@@ -349,8 +349,12 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
     V.xPrev = reinterpret_cast<float4*>(base + L.xPrev);
     V.xComp = COMP ? reinterpret_cast<float4*>(base + L.xComp) : A.xComp + R.pOff;
     V.qComp = COMP ? reinterpret_cast<float4*>(base + L.qComp) : A.qComp + R.sOff;
-    V.v = reinterpret_cast<float4*>(base + L.v);
-    V.omega = reinterpret_cast<float4*>(base + L.omega);
+    // velocities: none in shared memory (see the prediction below); the
+    // state arrays in global memory hold them between steps
+    V.v = nullptr;
+    V.omega = nullptr;
+    float4* const gv = A.v + R.pOff;
+    float4* const gw = A.omega + R.sOff;
     // multipliers: none at one iteration; else in global memory (L1/L2)
     V.lamS = A.iterations > 1 ? A.gLamS + R.stOff : nullptr;
     V.lamB = A.iterations > 1 ? A.gLamB + R.bOff : nullptr;
@@ -436,11 +440,9 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
     if (lane == 0) {
         C.stageFailed = 0;
         mbarInit(&C.bar);
-        mbarArriveExpectTx(&C.bar, 2u * pBytes + 2u * sBytes + (COMP ? pBytes + sBytes : 0u));
+        mbarArriveExpectTx(&C.bar, pBytes + sBytes + (COMP ? pBytes + sBytes : 0u));
         bulkLoad(V.x, A.x + R.pOff, pBytes, &C.bar);
-        bulkLoad(V.v, A.v + R.pOff, pBytes, &C.bar);
         bulkLoad(V.q, A.q + R.sOff, sBytes, &C.bar);
-        bulkLoad(V.omega, A.omega + R.sOff, sBytes, &C.bar);
         if (COMP) {
             bulkLoad(V.xComp, A.xComp + R.pOff, pBytes, &C.bar);
             bulkLoad(V.qComp, A.qComp + R.sOff, sBytes, &C.bar);
@@ -603,14 +605,17 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
             }
             // the previous substep's velocity update runs here, fused with this
             // substep's prediction: nothing between them reads v or omega,
-            // and each element's two updates stay with one thread
+            // and each element's two updates stay with one thread, so the
+            // velocities pass from the update to the prediction in registers;
+            // the prediction's own velocity is never read (the next update
+            // replaces it), so velocities are in memory only between steps
             for (int i = lane; i < nP; i += team) {
-                if (sub > 0) finishParticle<COMP>(V, i, h, A.linDecay);
-                predictParticle<COMP>(V, i, h, g);
+                const float4 vi = sub > 0 ? finishedVelocity<COMP>(V, i, h, A.linDecay) : gv[i];
+                predictParticleFrom<COMP>(V, i, h, g, vi, nullptr);
             }
             for (int j = lane; j < nS; j += team) {
-                if (sub > 0) finishFrame<COMP>(V, j, h, A.angDecay);
-                predictFrame<COMP>(V, j, h);
+                const float4 wj = sub > 0 ? finishedOmega<COMP>(V, j, h, A.angDecay) : gw[j];
+                predictFrameFrom<COMP>(V, j, h, wj, nullptr);
             }
             teamSync(team, teamIdx);
 
@@ -663,8 +668,8 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
 
         }
         // the step's last velocity update
-        for (int i = lane; i < nP; i += team) finishParticle<COMP>(V, i, h, A.linDecay);
-        for (int j = lane; j < nS; j += team) finishFrame<COMP>(V, j, h, A.angDecay);
+        for (int i = lane; i < nP; i += team) gv[i] = finishedVelocity<COMP>(V, i, h, A.linDecay);
+        for (int j = lane; j < nS; j += team) gw[j] = finishedOmega<COMP>(V, j, h, A.angDecay);
         teamSync(team, teamIdx);
 
         // ---- per-step bookkeeping ----
@@ -692,9 +697,7 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
     teamSync(team, teamIdx);
     if (lane == 0) {
         bulkStore(A.x + R.pOff, V.x, pBytes);
-        bulkStore(A.v + R.pOff, V.v, pBytes);
         bulkStore(A.q + R.sOff, V.q, sBytes);
-        bulkStore(A.omega + R.sOff, V.omega, sBytes);
         if (COMP) {
             bulkStore(A.xComp + R.pOff, V.xComp, pBytes);
             bulkStore(A.qComp + R.sOff, V.qComp, sBytes);

@@ -6,16 +6,19 @@
 // lean layout (batched kernel) keeps what every substep reads and writes --
 // positions and their start-of-substep copies, frames and (except under
 // compensation, where the shared memory is worth more as occupancy) their
-// start-of-substep copies, velocities, angular velocities, the self-contact
-// count's centres -- and leaves in global memory what a step only reads (loads,
-// kinematic velocities) or touches only when a contact is live (world
+// start-of-substep copies, the self-contact count's centres -- and leaves in
+// global memory what a step only reads (loads, kinematic velocities) or
+// touches only when a contact is live (world
 // contact slots of primitives that survive the per-rod cull, the
 // self-contact hash, sort, pool and projection levels); those stay
 // L1/L2-resident. `slotsShared` moves the
 // world contact slots into the lean layout too, for batches whose groups
-// still fit as many CTAs per SM with them.
-//   frames     q, qPrev (not lean+comp), omega [, torque]  16 x nS each
-//   particles  x, xPrev, v [, force, kin], xComp     16 x nP each (xComp: full,
+// still fit as many CTAs per SM with them. The lean layout holds no
+// velocities: within a step each lane carries its elements' velocities in
+// registers from the velocity update into the next prediction, and between
+// steps they are in the global state arrays.
+//   frames     q, qPrev (not lean+comp), omega (full) [, torque]  16 x nS each
+//   particles  x, xPrev, v (full) [, force, kin], xComp  16 x nP each (xComp: full,
 //                                                    or lean with compensation)
 //   frames     qComp                                 16 x nS (lean with compensation)
 //   lambdas    stretch, bend                         16 x (nSt + nB) (full only: the
@@ -72,8 +75,12 @@ RP_HD inline RodLayout rodLayout(int32_t nP, int32_t nS, int32_t nSt, int32_t nB
     }
     L.x = o;      o += 16 * nP;
     L.xPrev = o;  o += 16 * nP;
-    L.omega = o;  o += 16 * nS;
-    L.v = o;      o += 16 * nP;
+    if (!lean) {  // lean: velocities stay in registers within a step
+        L.omega = o;  o += 16 * nS;
+        L.v = o;      o += 16 * nP;
+    } else {
+        L.omega = L.v = -1;
+    }
     if (!lean) {
         L.torque = o; o += 16 * nS;
         L.force = o;  o += 16 * nP;

@@ -639,32 +639,44 @@ __device__ __forceinline__ void projectSelf(const RodView& V, DSelf& c) {
 
 // ---------------------------------------------------------------- predict / finish
 
+// Prediction of particle i from the velocity vIn. The predicted velocity is
+// written to *vOut when it is given: the plain kernel keeps it in its state
+// array; the batched kernel drops it, because the substep's velocity update
+// replaces it without reading it.
 template <bool COMP>
-__device__ __forceinline__ void predictParticle(const RodView& V, int i, float h, V3 g) {
+__device__ __forceinline__ void predictParticleFrom(const RodView& V, int i, float h, V3 g, float4 vIn,
+                                                    float4* vOut) {
     V.xPrev[i] = COMP ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : V.x[i];
     const float w = V.g->invMass[i];
     if (w == 0.0f) {
         addPos<COMP>(V, i, v3(V.g->kin[i]), h);  // prescribed motion
         return;
     }
-    const V3 vn = fmav(fmav(v3(V.g->force[i]), w, g), h, v3(V.v[i]));  // v + (g + f w) h
-    V.v[i] = f4(vn);
+    const V3 vn = fmav(fmav(v3(V.g->force[i]), w, g), h, v3(vIn));  // v + (g + f w) h
+    if (vOut) *vOut = f4(vn);
     addPos<COMP>(V, i, vn, h);
 }
 
 template <bool COMP>
-__device__ __forceinline__ void predictFrame(const RodView& V, int j, float h) {
+__device__ __forceinline__ void predictParticle(const RodView& V, int i, float h, V3 g) {
+    predictParticleFrom<COMP>(V, i, h, g, V.v[i], &V.v[i]);
+}
+
+// Prediction of frame j from the angular velocity wIn (*wOut as for the
+// particles).
+template <bool COMP>
+__device__ __forceinline__ void predictFrameFrom(const RodView& V, int j, float h, float4 wIn, float4* wOut) {
     const float4 qs = V.q[j];
     // compensated: the substep's accumulated rotation starts at identity
     V.qPrev[j] = COMP ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : qs;
     const V3 iI = v3(V.g->invInertia[j]);
     if (norm2(iI) == 0.0f) return;
     if (COMP) renormalizeFrameComp(V, j);  // once per substep, in FP64
-    const V3 w = v3(V.omega[j]);
+    const V3 w = v3(wIn);
     const Q4 q = q4(V.q[j]);
     const V3 tau = rotateInv(q, v3(V.g->torque[j]));
     const V3 wn = fmav(cwise(iI, tau - cross(w, cwise(v3(V.g->inertia[j]), w))), h, w);
-    V.omega[j] = f4(wn);
+    if (wOut) *wOut = f4(wn);
     if (COMP)
         rotateFrameComp(V, j, wn * (0.5f * h));
     else
@@ -672,21 +684,29 @@ __device__ __forceinline__ void predictFrame(const RodView& V, int j, float h) {
 }
 
 template <bool COMP>
-__device__ __forceinline__ void finishParticle(const RodView& V, int i, float h, float linDecay) {
-    if (V.g->invMass[i] == 0.0f) {
-        V.v[i] = V.g->kin[i];
-        return;
-    }
+__device__ __forceinline__ void predictFrame(const RodView& V, int j, float h) {
+    predictFrameFrom<COMP>(V, j, h, V.omega[j], &V.omega[j]);
+}
+
+// Velocity of particle i at the end of a substep (recovered from its
+// displacement; a kinematic particle takes its prescribed velocity).
+template <bool COMP>
+__device__ __forceinline__ float4 finishedVelocity(const RodView& V, int i, float h, float linDecay) {
+    if (V.g->invMass[i] == 0.0f) return V.g->kin[i];
     const V3 d = dispOf<COMP>(V, i);
-    V.v[i] = f4(divs(d, h) * linDecay);
+    return f4(divs(d, h) * linDecay);
 }
 
 template <bool COMP>
-__device__ __forceinline__ void finishFrame(const RodView& V, int j, float h, float angDecay) {
-    if (norm2(v3(V.g->invInertia[j])) == 0.0f) {
-        V.omega[j] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        return;
-    }
+__device__ __forceinline__ void finishParticle(const RodView& V, int i, float h, float linDecay) {
+    V.v[i] = finishedVelocity<COMP>(V, i, h, linDecay);
+}
+
+// Angular velocity of frame j at the end of a substep (from the substep's
+// rotation; a frame with no inverse inertia is at rest).
+template <bool COMP>
+__device__ __forceinline__ float4 finishedOmega(const RodView& V, int j, float h, float angDecay) {
+    if (norm2(v3(V.g->invInertia[j])) == 0.0f) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     Q4 dq;
     if (COMP) {
         const Q4 e = q4(V.qPrev[j]);  // the substep's rotation 1 + e
@@ -694,7 +714,12 @@ __device__ __forceinline__ void finishFrame(const RodView& V, int j, float h, fl
     } else {
         dq = sameHemisphereId(qmulConj(q4(V.qPrev[j]), q4(V.q[j])));
     }
-    V.omega[j] = f4(im(dq) * (2.0f / h) * angDecay);
+    return f4(im(dq) * (2.0f / h) * angDecay);
+}
+
+template <bool COMP>
+__device__ __forceinline__ void finishFrame(const RodView& V, int j, float h, float angDecay) {
+    V.omega[j] = finishedOmega<COMP>(V, j, h, angDecay);
 }
 
 // ---------------------------------------------------------------- waypoint drives

@@ -4,8 +4,9 @@
   index gap) with self-collision and a floor on: every strategy gives the same
   state bit for bit, and the FP64 oracle agrees to 1e-5 of the rod length
   after a few steps.
-* A 3000-segment rod exceeds the batched kernel's shared memory: the batched
-  strategy refuses it with RP_ERR_SHARED_MEMORY and a message, the
+* A 3000-segment rod fits the batched kernel's shared memory and steps
+  bitwise equal to the multi-kernel strategy; a 4000-segment rod exceeds it:
+  the batched strategy refuses it with RP_ERR_SHARED_MEMORY and a message, the
   multi-kernel strategy (state in global memory) steps it and agrees with the
   FP64 oracle.
 * A world with 64 primitives (the maximum) steps identically under every
@@ -55,9 +56,29 @@ def test_shortest_rods(oracle64, segments):
     assert np.max(np.abs(got - o.x[: o.nP])) <= 1e-5 * 0.02 * segments + 1e-7
 
 
-def test_longest_rod_multi_kernel_only(oracle64):
+def test_longest_rods(oracle64):
+    # 3000 segments: the batched kernel's lean layout (positions and frames
+    # with their start-of-substep copies, 64 bytes a segment without
+    # self-collision) fits one CTA's shared memory; its 256-thread team
+    # projects several constraints of a colour per lane, in pairs
     n = 3000
     o = oracle64.straight(n, 3.0, youngs=1e8, poisson=0.3, density=1100.0, radius=5e-3)
+    oracle64.clamp(o, False)
+    proto = product_rod(o)
+    out = {}
+    for s in (rp.Strategy.BATCHED, rp.Strategy.MULTI_KERNEL):
+        b = rp.Batch.create(proto, 1, s)
+        b.step_many(P, 3)
+        out[s] = (b.download_positions().reshape(-1, 3), b.download_frames())
+        b.close()
+    assert np.array_equal(out[rp.Strategy.BATCHED][0], out[rp.Strategy.MULTI_KERNEL][0])
+    assert np.array_equal(out[rp.Strategy.BATCHED][1], out[rp.Strategy.MULTI_KERNEL][1])
+    oracle64.step(o, OPAR, steps=3)
+    assert np.max(np.abs(out[rp.Strategy.MULTI_KERNEL][0] - o.x[: o.nP])) <= 1e-5 * 3.0
+    # 4000 segments exceed it: the batched strategy refuses the rod, the
+    # multi-kernel strategy (state in global memory) steps it
+    n = 4000
+    o = oracle64.straight(n, 4.0, youngs=1e8, poisson=0.3, density=1100.0, radius=5e-3)
     oracle64.clamp(o, False)
     proto = product_rod(o)
     with pytest.raises(rp.RopeError) as e:
@@ -68,7 +89,7 @@ def test_longest_rod_multi_kernel_only(oracle64):
     x = b.download_positions().reshape(-1, 3)
     b.close()
     oracle64.step(o, OPAR, steps=3)
-    assert np.max(np.abs(x - o.x[: o.nP])) <= 1e-5 * 3.0
+    assert np.max(np.abs(x - o.x[: o.nP])) <= 1e-5 * 4.0
 
 
 def test_sixty_four_primitives():
@@ -95,7 +116,7 @@ def test_refused_precision_change_keeps_the_plan(oracle64):
     batch that never tried. The length is the first of a ladder that splits
     the two layouts on this device."""
     proto = b = smem = None
-    for n in range(1500, 3001, 100):
+    for n in range(2000, 4001, 100):
         o = oracle64.straight(n, n / 1000.0, youngs=1e8, poisson=0.3, density=1100.0, radius=5e-3)
         oracle64.clamp(o, False)
         cand = product_rod(o)
