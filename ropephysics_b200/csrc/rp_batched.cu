@@ -120,7 +120,10 @@ __device__ __forceinline__ int bucketMultiplicity(float4 cj, float4 ck, float ce
     return m;
 }
 
-// segCount[j] (zeroed by the caller) += the reference's count of segment j.
+// segCount[j] (zeroed by the caller) += the reference's count of segment j;
+// every touching pair (j, k) is also appended to pairList as (j << 16) | k
+// (*numPairs, zeroed by the caller, counts them; entries past nSt are not
+// stored).
 // Warp w of the team takes chain blocks J = w, w + warps, ...; its lanes test
 // 32 blocks K >= J at a time against J by box distance, and for each block
 // that can hold a pair within the sphere bound the warp runs the 64 segment
@@ -130,7 +133,8 @@ __device__ __forceinline__ int bucketMultiplicity(float4 cj, float4 ck, float ce
 // by its block maximum (float max, add and multiply are monotone), so every
 // pair the sphere test keeps is reached.
 __device__ void countSelfByBlocks(const RodView& V, const SelfScratch& S, int nSt, int gap, int table,
-                                  float cell, int lane, int team, int32_t* touching) {
+                                  float cell, int lane, int team, int32_t* touching, int32_t* pairList,
+                                  int32_t* numPairs) {
     if (nSt <= gap) return;
     const int wl = lane & 31, warp = lane >> 5, warps = team >> 5;
     const int nBlk = (nSt + 7) >> 3;
@@ -173,6 +177,11 @@ __device__ void countSelfByBlocks(const RodView& V, const SelfScratch& S, int nS
                     if (mult) {
                         atomicAdd(&S.segCount[j], mult);
                         *touching = 1;
+                        // the touching pair, for the pool built from pairs;
+                        // the list holds nSt pairs, beyond that the count
+                        // alone is kept and the pool is built from the hash
+                        const int at = atomicAdd(numPairs, 1);
+                        if (at < nSt) pairList[at] = (j << 16) | k;
                     }
                 }
             }
@@ -219,6 +228,33 @@ constexpr int32_t kErrorStage = 2;
 // One context per team: a 256-thread CTA holds at most eight one-warp teams.
 constexpr int kMaxTeamsPerCta = 8;
 
+// The projection levels (or colours) of a filled pool of `live` entries, by
+// one thread. S.cellOf serves as the per-particle scratch and must be zero
+// at every particle of the pool.
+__device__ void buildPoolLevels(const TeamCtx& C, int nP, int live, int precision, int32_t* errorWord) {
+    const SelfScratch& S = C.S;
+    int kept = live;
+    int n = buildProjectionLevels(S.pool, live, nP, S.cellOf, C.lvlOf, C.lvlOrder, C.lvlStart, &kept);
+    if (precision & kPrecisionColoredSelf) {
+        // colours instead of levels (the valid prefix is known now)
+        for (int i = 0; i < nP; ++i) S.cellOf[i] = 0;
+        const int nc = buildProjectionColors(S.pool, kept, S.cellOf, C.lvlOf, C.lvlOrder, C.lvlStart);
+        if (nc >= 0) {
+            n = nc;
+        } else {  // more than 32 colours: keep the levels
+            for (int i = 0; i < nP; ++i) S.cellOf[i] = 0;
+            n = buildProjectionLevels(S.pool, kept, nP, S.cellOf, C.lvlOf, C.lvlOrder, C.lvlStart, &kept);
+        }
+    }
+    *C.numLevels = n;
+    if (kept != live) {
+        // an entry indexed outside the rod or left unwritten: keep the
+        // valid prefix and report it, never touch memory with it
+        *S.live = kept;
+        if (errorWord) atomicOr(errorWord, 1);
+    }
+}
+
 // The pool fill of a substep on which some segment pair touches: the
 // reference's hash (a stable counting sort), its fill pass in bucket order,
 // and the projection levels (or colours) of the pool. Not inlined: it runs
@@ -231,10 +267,6 @@ __device__ __noinline__ void fillSelfPool(const TeamCtx& C, int nSt, int nP, int
     const SelfScratch& S = C.S;
     int32_t* const& cursor = C.cursor;
     int32_t* const& partial = C.partial;
-    int32_t* const& numLevels = C.numLevels;
-    int32_t* const& lvlOrder = C.lvlOrder;
-    int32_t* const& lvlStart = C.lvlStart;
-    int32_t* const& lvlOf = C.lvlOf;
         // ---- fill, in the reference's order: its hash buckets ----
         for (int t = lane; t <= table; t += team) S.cellStart[t] = 0;
         for (int c = lane; c < live; c += team) S.pool[c].seg = -1;
@@ -279,32 +311,82 @@ __device__ __noinline__ void fillSelfPool(const TeamCtx& C, int nSt, int nP, int
         teamSync(team, teamIdx);
         for (int i = lane; i < nP; i += team) S.cellOf[i] = 0;
         teamSync(team, teamIdx);
-        if (lane == 0) {
-            int kept = live;
-            int n = buildProjectionLevels(S.pool, live, nP, S.cellOf, lvlOf, lvlOrder,
-                                          lvlStart, &kept);
-            if (precision & kPrecisionColoredSelf) {
-                // colours instead of levels (the valid prefix is known now)
-                for (int i = 0; i < nP; ++i) S.cellOf[i] = 0;
-                const int nc = buildProjectionColors(S.pool, kept, S.cellOf, lvlOf, lvlOrder,
-                                                     lvlStart);
-                if (nc >= 0) {
-                    n = nc;
-                } else {  // more than 32 colours: keep the levels
-                    for (int i = 0; i < nP; ++i) S.cellOf[i] = 0;
-                    n = buildProjectionLevels(S.pool, kept, nP, S.cellOf, lvlOf, lvlOrder,
-                                              lvlStart, &kept);
-                }
+        if (lane == 0) buildPoolLevels(C, nP, live, precision, errorWord);
+}
+
+// Bits t = 9 (dz + 1) + 3 (dy + 1) + (dx + 1) of the 27 cells around
+// cell(j) whose hash is k's bucket hash(cell(k)): the cells, in the
+// reference's query order, at which its query meets k.
+__device__ __forceinline__ unsigned bucketCells(float4 cj, float4 ck, float cell, int table) {
+    const int cx = cellCoord(cj.x, cell), cy = cellCoord(cj.y, cell), cz = cellCoord(cj.z, cell);
+    const unsigned hk = hashCell(cellCoord(ck.x, cell), cellCoord(ck.y, cell), cellCoord(ck.z, cell), table);
+    unsigned m = 0u;
+    int t = 0;
+    for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx, ++t)
+                if (hashCell(cx + dx, cy + dy, cz + dz, table) == hk) m |= 1u << t;
+    return m;
+}
+
+// Most touching substeps have a handful of touching pairs; for those the
+// pool is built from the count's pair list by the team's first warp, with
+// no hash. The reference's query for segment j walks the 27 cells around
+// cell(j) in order and, in each, the bucket of that cell's hash in segment
+// order, so its pool holds one entry per touching pair (j, k) and per cell t
+// whose hash is k's bucket, ordered by (j, t, k), and segment j's entries
+// start after every entry of the segments before it. Each lane takes one
+// pair, finds its cells, ranks each of its entries by counting the entries
+// of every pair that order before it, and writes them with the query's own
+// entry writer: the same pool, entry for entry. Lanes past the capacity
+// write nothing, as the query does. Every lane of the warp calls this; it
+// returns the reference's count of entries. The pair list is
+// S.segStart[0..numPairs), numPairs <= 32; S.segCount holds the pairs' cell
+// masks afterwards, and S.cellOf is zeroed at the pool's particles for the
+// level build.
+__device__ __noinline__ int poolFromPairs(const TeamCtx& C, int numPairs, int table, float cell,
+                                          int selfCapacity, float selfFriction, int lane) {
+    const RodView& V = C.V;
+    const SelfScratch& S = C.S;
+    const bool mine = lane < numPairs;
+    int j = 0, k = 0;
+    unsigned cells = 0u;
+    if (mine) {
+        const int pr = S.segStart[lane];
+        j = pr >> 16;
+        k = pr & 0xffff;
+        cells = bucketCells(S.centres[j], S.centres[k], cell, table);
+    }
+    const int total = __reduce_add_sync(0xffffffffu, __popc(cells));
+    __syncwarp();
+    if (mine) S.segCount[lane] = int32_t(cells);
+    __syncwarp();
+    if (mine) {
+        const int p0 = V.g->sP0[j], p1 = V.g->sP1[j], p2 = V.g->sP0[k], p3 = V.g->sP1[k];
+        S.cellOf[p0] = 0;
+        S.cellOf[p1] = 0;
+        S.cellOf[p2] = 0;
+        S.cellOf[p3] = 0;
+        const SegPair P = segmentPairNarrow(v3(V.x[p0]), v3(V.x[p1]), v3(V.x[p2]), v3(V.x[p3]),
+                                            2.0f * V.radius);
+        // entries of the pairs of earlier segments
+        int before = 0;
+        for (int q = 0; q < numPairs; ++q)
+            if ((S.segStart[q] >> 16) < j) before += __popc(unsigned(S.segCount[q]));
+        for (unsigned rest = cells; rest; rest &= rest - 1u) {
+            const int t = __ffs(rest) - 1;
+            const unsigned below = (1u << t) - 1u;
+            int rank = before;
+            for (int q = 0; q < numPairs; ++q) {
+                const int pq = S.segStart[q];
+                if ((pq >> 16) != j) continue;
+                const unsigned cq = unsigned(S.segCount[q]);
+                rank += __popc(cq & below) + (((cq >> t) & 1u) && (pq & 0xffff) < k ? 1 : 0);
             }
-            *numLevels = n;
-            if (kept != live) {
-                // an entry indexed outside the rod or left unwritten:
-                // keep the valid prefix and report it, never touch
-                // memory with it
-                *S.live = kept;
-                if (errorWord) atomicOr(errorWord, 1);
-            }
+            if (rank < selfCapacity) writeSelfEntry(V, S.pool[rank], j, k, P, selfFriction);
         }
+    }
+    return total;
 }
 
 // The self-contact pool projected level by level: contacts of one level
@@ -377,6 +459,7 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
     int32_t* numLevels = misc + 3;
     unsigned long long* primMask = reinterpret_cast<unsigned long long*>(misc + 12);
     int32_t* touching = misc + 14;
+    int32_t* numPairs = misc + 15;
     float* red = reinterpret_cast<float*>(misc + 16);  // 8 floats per warp
     if (lane == 0) {
         RodGlobals& G = C.G;
@@ -543,7 +626,10 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
                     row[4] = hx; row[5] = hy; row[6] = hz;
                 }
                 // reset before the barrier: the count below follows without one
-                if (lane == 0) *touching = 0;
+                if (lane == 0) {
+                    *touching = 0;
+                    *numPairs = 0;
+                }
                 teamSync(team, teamIdx);  // centres, blocks, zeroed counts, rows visible
                 // every lane reduces the rows in the same order (max and min
                 // are exact), so every lane holds the same mask and cell size;
@@ -572,24 +658,42 @@ __device__ void runRod(const DArgs& A, int r, unsigned char* base, int lane, int
                     const float cell = cellNow;
                     // ---- count: contacts per segment, by chain blocks ----
                     // chain-block bounds and zeroed counts come from the centre pass
-                    countSelfByBlocks(V, S, nSt, R.selfGap, table, cell, lane, team, touching);
+                    // the pair list takes segStart, which the hash path rebuilds
+                    countSelfByBlocks(V, S, nSt, R.selfGap, table, cell, lane, team, touching, S.segStart,
+                                      numPairs);
                     teamSync(team, teamIdx);
-                    int total = 0;
-                    if (*touching) {  // team-uniform: one shared word read after the barrier
-                        for (int j = lane; j < nSt; j += team) S.segStart[j] = S.segCount[j];
-                        teamSync(team, teamIdx);
-                        total = teamExclusiveScan(S.segStart, nSt, lane, team, teamIdx, partial);
-                    }
-                    const int live = total < R.selfCapacity ? total : R.selfCapacity;
-                    if (lane == 0) {
-                        *S.live = live;
-                        if (total > R.selfCapacity) *S.overflow += total - R.selfCapacity;
-                    }
-                    if (live > 0) {
-                        fillSelfPool(C, nSt, nP, table, cell, live, R.selfGap, R.selfCapacity, R.selfFriction, A.precision,
-                                     A.errors ? A.errors + r : nullptr, lane, team, teamIdx);
-                    } else if (lane == 0) {
-                        *numLevels = 0;
+                    // team-uniform: shared words read after the barrier
+                    const int pairs = *touching ? *numPairs : 0;
+                    if (pairs > 0 && pairs <= 32 && pairs <= nSt) {
+                        int total = 0;
+                        if (lane < 32)
+                            total = poolFromPairs(C, pairs, table, cell, R.selfCapacity, R.selfFriction, lane);
+                        const int live = total < R.selfCapacity ? total : R.selfCapacity;
+                        if (lane == 0) {
+                            *S.live = live;
+                            if (total > R.selfCapacity) *S.overflow += total - R.selfCapacity;
+                        }
+                        teamSync(team, teamIdx);  // pool written, positions read: the prediction may start
+                        if (lane == 0)
+                            buildPoolLevels(C, nP, live, A.precision, A.errors ? A.errors + r : nullptr);
+                    } else {
+                        int total = 0;
+                        if (pairs > 0) {
+                            for (int j = lane; j < nSt; j += team) S.segStart[j] = S.segCount[j];
+                            teamSync(team, teamIdx);
+                            total = teamExclusiveScan(S.segStart, nSt, lane, team, teamIdx, partial);
+                        }
+                        const int live = total < R.selfCapacity ? total : R.selfCapacity;
+                        if (lane == 0) {
+                            *S.live = live;
+                            if (total > R.selfCapacity) *S.overflow += total - R.selfCapacity;
+                        }
+                        if (live > 0) {
+                            fillSelfPool(C, nSt, nP, table, cell, live, R.selfGap, R.selfCapacity, R.selfFriction,
+                                         A.precision, A.errors ? A.errors + r : nullptr, lane, team, teamIdx);
+                        } else if (lane == 0) {
+                            *numLevels = 0;
+                        }
                     }
                 } else if (lane == 0) {
                     for (int c = 0; c < *S.live; ++c) {

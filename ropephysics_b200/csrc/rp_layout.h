@@ -57,6 +57,7 @@ struct RodLayout {
 //   [0] cell size  [1] live pool entries  [2] overflow  [3] projection levels
 //   [4..11] per-warp scan partials  [12..13] primitive mask (64 bits)
 //   [14] a self-contact pair touches this substep (batched)
+//   [15] touching pairs found by the count (batched)
 //   [16..79] per-warp reduction rows (8 warps x 8 floats)
 constexpr int32_t kMiscBytes = 320;
 

@@ -450,6 +450,35 @@ static __device__ __noinline__ SegPair segmentPairNarrow(V3 a0, V3 a1, V3 b0, V3
     return r;
 }
 
+// The pool entry of touching segments j < k from their narrow phase P: the
+// contact normal, the four particles and their weights, the offset from the
+// current positions, friction, zeroed multipliers and the pair id.
+__device__ __forceinline__ void writeSelfEntry(const RodView& V, DSelf& c, int j, int k, const SegPair& P,
+                                               float selfFriction) {
+    const float u = P.u, w = P.w, dist = P.dist, separation = P.separation;
+    const V3 delta = P.delta;
+    const V3 n = dist > 1e-12f ? divs(delta, dist) : V3{0.0f, 0.0f, 1.0f};
+    c.nx = n.x;
+    c.ny = n.y;
+    c.nz = n.z;
+    c.idx[0] = V.g->sP0[j];
+    c.idx[1] = V.g->sP1[j];
+    c.idx[2] = V.g->sP0[k];
+    c.idx[3] = V.g->sP1[k];
+    c.weight[0] = 1.0f - u;
+    c.weight[1] = u;
+    c.weight[2] = -(1.0f - w);
+    c.weight[3] = -w;
+    float dotSum = 0.0f;
+    for (int m = 0; m < 4; ++m)
+        dotSum = fma3(c.weight[m], dot(v3(V.x[c.idx[m]]), n), dotSum);
+    c.offset = dotSum - separation;
+    c.friction = selfFriction * V.frictionScale;
+    c.lambdaN = 0.0f;
+    c.applied = 0.0f;
+    c.seg = (j << 16) | k;
+}
+
 // Contacts of segment j with later segments, in the reference's candidate
 // order (3x3x3 cells z/y/x, bucket order within a cell). fill = false counts
 // them into segCount[j]; fill = true writes them from segStart[j].
@@ -491,32 +520,10 @@ __device__ __forceinline__ void querySelfSegment(const RodView& V, const SelfScr
                         const V3 b0 = v3(V.x[V.g->sP0[k]]), b1 = v3(V.x[V.g->sP1[k]]);
                         const SegPair P = segmentPairNarrow(a0, a1, b0, b1, twoR);
                         if (P.separation >= 0.0f) continue;
-                        const float u = P.u, w = P.w, dist = P.dist, separation = P.separation;
-                        const V3 delta = P.delta;
                         const int slot = fill ? S.segStart[j] + count : 0;
                         ++count;
                         if (!fill || slot >= capacity) continue;
-                        DSelf& c = S.pool[slot];
-                        const V3 n = dist > 1e-12f ? divs(delta, dist) : V3{0.0f, 0.0f, 1.0f};
-                        c.nx = n.x;
-                        c.ny = n.y;
-                        c.nz = n.z;
-                        c.idx[0] = V.g->sP0[j];
-                        c.idx[1] = V.g->sP1[j];
-                        c.idx[2] = V.g->sP0[k];
-                        c.idx[3] = V.g->sP1[k];
-                        c.weight[0] = 1.0f - u;
-                        c.weight[1] = u;
-                        c.weight[2] = -(1.0f - w);
-                        c.weight[3] = -w;
-                        float dotSum = 0.0f;
-                        for (int m = 0; m < 4; ++m)
-                            dotSum = fma3(c.weight[m], dot(v3(V.x[c.idx[m]]), n), dotSum);
-                        c.offset = dotSum - separation;
-                        c.friction = selfFriction * V.frictionScale;
-                        c.lambdaN = 0.0f;
-                        c.applied = 0.0f;
-                        c.seg = (j << 16) | k;
+                        writeSelfEntry(V, S.pool[slot], j, k, P, selfFriction);
                     }
                 }
     }
