@@ -132,6 +132,26 @@ __device__ __forceinline__ int bucketMultiplicity(float4 cj, float4 ck, float ce
 // when box distance^2 > 1.0001 x bound^2 with every per-pair quantity bounded
 // by its block maximum (float max, add and multiply are monotone), so every
 // pair the sphere test keeps is reached.
+// A pair that passed the sphere test: the shared narrow phase, and for a
+// touching pair its bucket multiplicity, its count and its place in the pair
+// list (which holds nSt pairs; beyond that the count alone is kept and the
+// pool is built from the hash). Not inlined: few pairs get here, and its
+// body is shared by every caller.
+__device__ __noinline__ void countTouching(const RodView& V, const SelfScratch& S, int j, int k, float4 cj,
+                                           float4 ck, float twoR, float cell, int table, int nSt,
+                                           int32_t* touching, int32_t* pairList, int32_t* numPairs) {
+    const SegPair P = segmentPairNarrow(v3(V.x[V.g->sP0[j]]), v3(V.x[V.g->sP1[j]]), v3(V.x[V.g->sP0[k]]),
+                                        v3(V.x[V.g->sP1[k]]), twoR);
+    if (P.separation >= 0.0f) return;
+    const int mult = bucketMultiplicity(cj, ck, cell, table);
+    if (mult) {
+        atomicAdd(&S.segCount[j], mult);
+        *touching = 1;
+        const int at = atomicAdd(numPairs, 1);
+        if (at < nSt) pairList[at] = (j << 16) | k;
+    }
+}
+
 __device__ void countSelfByBlocks(const RodView& V, const SelfScratch& S, int nSt, int gap, int table,
                                   float cell, int lane, int team, int32_t* touching, int32_t* pairList,
                                   int32_t* numPairs) {
@@ -139,14 +159,55 @@ __device__ void countSelfByBlocks(const RodView& V, const SelfScratch& S, int nS
     const int wl = lane & 31, warp = lane >> 5, warps = team >> 5;
     const int nBlk = (nSt + 7) >> 3;
     const float twoR = 2.0f * V.radius;
+    // This lane's pair of the block with itself, for the near pairs: the 28
+    // pairs (a, b), a < b, of a block ordered by b - a descending, so the
+    // pairs with b - a >= gap are a prefix (28 of them for gap 1, 15 for 3).
+    int ta = -1, tb = -1;
+    {
+        int e = wl;
+        for (int d = 7; d >= 1; --d) {
+            if (e < 8 - d) {
+                ta = e;
+                tb = e + d;
+                break;
+            }
+            e -= 8 - d;
+        }
+    }
     for (int J = warp; J < nBlk; J += warps) {
         const float4 jlo = S.blocks[2 * J], jhi = S.blocks[2 * J + 1];
         const int jmin = 8 * J;
-        // this lane's segment of J for the pair tests
+        // this lane's segment of J for the pair tests against other blocks
         const int j = jmin + (wl & 7);
         const float4 cj = j < nSt ? S.centres[j] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         const float scaleSlack = 1e-6f * (1.0f + fabsf(cj.x) + fabsf(cj.y) + fabsf(cj.z));
-        for (int K0 = J; K0 < nBlk; K0 += 32) {
+        // The per-pair test: the sphere test of querySelfSegment, then the
+        // narrow phase and the count for the pairs that pass.
+        auto testPair = [&](int pj, int pk, float4 pcj, float pslack) {
+            const float4 ck = S.centres[pk];
+            const float ddx = ck.x - pcj.x, ddy = ck.y - pcj.y, ddz = ck.z - pcj.z;
+            const float bound = pcj.w + ck.w + twoR;
+            const float plim = bound * 1.001f + pslack;
+            if (ddx * ddx + ddy * ddy + ddz * ddz > plim * plim) return;
+            countTouching(V, S, pj, pk, pcj, ck, twoR, cell, table, nSt, touching, pairList, numPairs);
+        };
+        // Near pairs, with no box test (the boxes of J and J + 1 always
+        // meet): J against J + 1 in two rounds of 32, J against itself in one
+        // round over the pairs with b - a >= gap.
+        if (J + 1 < nBlk) {
+#pragma unroll
+            for (int h2 = 0; h2 < 2; ++h2) {
+                const int k = 8 * (J + 1) + (wl >> 3) + 4 * h2;
+                if (j < nSt && k < nSt && k - j >= gap) testPair(j, k, cj, scaleSlack);
+            }
+        }
+        if (ta >= 0 && tb - ta >= gap && jmin + tb < nSt) {
+            const int j2 = jmin + ta;
+            const float4 cj2 = S.centres[j2];
+            testPair(j2, jmin + tb, cj2, 1e-6f * (1.0f + fabsf(cj2.x) + fabsf(cj2.y) + fabsf(cj2.z)));
+        }
+        // Blocks K >= J + 2, by box distance, 32 at a time.
+        for (int K0 = J + 2; K0 < nBlk; K0 += 32) {
             const int K = K0 + wl;
             bool hit = false;
             if (K < nBlk && min(8 * K + 7, nSt - 1) - jmin >= gap) {
@@ -164,25 +225,7 @@ __device__ void countSelfByBlocks(const RodView& V, const SelfScratch& S, int nS
 #pragma unroll
                 for (int h2 = 0; h2 < 2; ++h2) {
                     const int k = 8 * Kh + (wl >> 3) + 4 * h2;
-                    if (j >= nSt || k >= nSt || k - j < gap) continue;
-                    const float4 ck = S.centres[k];
-                    const float ddx = ck.x - cj.x, ddy = ck.y - cj.y, ddz = ck.z - cj.z;
-                    const float bound = cj.w + ck.w + twoR;
-                    const float plim = bound * 1.001f + scaleSlack;
-                    if (ddx * ddx + ddy * ddy + ddz * ddz > plim * plim) continue;
-                    const SegPair P = segmentPairNarrow(v3(V.x[V.g->sP0[j]]), v3(V.x[V.g->sP1[j]]),
-                                                        v3(V.x[V.g->sP0[k]]), v3(V.x[V.g->sP1[k]]), twoR);
-                    if (P.separation >= 0.0f) continue;
-                    const int mult = bucketMultiplicity(cj, ck, cell, table);
-                    if (mult) {
-                        atomicAdd(&S.segCount[j], mult);
-                        *touching = 1;
-                        // the touching pair, for the pool built from pairs;
-                        // the list holds nSt pairs, beyond that the count
-                        // alone is kept and the pool is built from the hash
-                        const int at = atomicAdd(numPairs, 1);
-                        if (at < nSt) pairList[at] = (j << 16) | k;
-                    }
+                    if (j < nSt && k < nSt && k - j >= gap) testPair(j, k, cj, scaleSlack);
                 }
             }
         }
