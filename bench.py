@@ -50,8 +50,8 @@ FLOPS_PER_SEG_SUBSTEP = {"uneven": 1696.2, "hook": 1446.1, "grid": 890.5, "canti
 BYTES_PER_SEG_STEP = 7 * 16 + 4 * 16
 # Measured DRAM bytes (read + write) per segment-step of the batched step,
 # from one ncu capture of a 4096-rod uneven batch (state beyond L2, so the
-# figure scales with segments: 244.6 MB over 1 084 256 segments).
-DRAM_BYTES_PER_SEG_STEP = {"uneven": 225.6}
+# figure scales with segments: 246.0 MB over 1 084 256 segments).
+DRAM_BYTES_PER_SEG_STEP = {"uneven": 226.9}
 
 
 def measured_peaks():
