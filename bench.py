@@ -10,8 +10,9 @@ the batched-vs-plain ratio. Metric: segment-substeps/s.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--workload uneven|grid]
   python bench.py --impl reference ...     # the reference's CPU solver, host cores
 
-Under torchrun every rank simulates its own seeded workload on its own GPU
-(rods are independent: weak scaling, no data-path collective); the time is the
+Under torchrun, rank r of N simulates shard r of one seeded uneven batch of
+N x 16384 rods on its own GPU (rods are independent: weak scaling, no
+data-path collective); the other workloads run as replicas. The time is the
 max over ranks.
 """
 from __future__ import annotations
