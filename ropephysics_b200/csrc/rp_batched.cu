@@ -108,16 +108,25 @@ __device__ int teamExclusiveScan(int32_t* a, int m, int lane, int team, int team
     return total;
 }
 
+// Bits t = 9 (dz + 1) + 3 (dy + 1) + (dx + 1) of the 27 cells around
+// cell(j) whose hash is k's bucket hash(cell(k)): the cells, in the
+// reference's query order, at which its query meets k.
+__device__ __forceinline__ unsigned bucketCells(float4 cj, float4 ck, float cell, int table) {
+    const int cx = cellCoord(cj.x, cell), cy = cellCoord(cj.y, cell), cz = cellCoord(cj.z, cell);
+    const unsigned hk = hashCell(cellCoord(ck.x, cell), cellCoord(ck.y, cell), cellCoord(ck.z, cell), table);
+    unsigned m = 0u;
+    int t = 0;
+    for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx, ++t)
+                if (hashCell(cx + dx, cy + dy, cz + dz, table) == hk) m |= 1u << t;
+    return m;
+}
+
 // Multiplicity of a touching pair in the reference's count: the number of
 // the 27 cells around cell(j) whose hash is k's bucket hash(cell(k)).
 __device__ __forceinline__ int bucketMultiplicity(float4 cj, float4 ck, float cell, int table) {
-    const int cx = cellCoord(cj.x, cell), cy = cellCoord(cj.y, cell), cz = cellCoord(cj.z, cell);
-    const unsigned hk = hashCell(cellCoord(ck.x, cell), cellCoord(ck.y, cell), cellCoord(ck.z, cell), table);
-    int m = 0;
-    for (int dz = -1; dz <= 1; ++dz)
-        for (int dy = -1; dy <= 1; ++dy)
-            for (int dx = -1; dx <= 1; ++dx) m += hashCell(cx + dx, cy + dy, cz + dz, table) == hk ? 1 : 0;
-    return m;
+    return __popc(bucketCells(cj, ck, cell, table));
 }
 
 // segCount[j] (zeroed by the caller) += the reference's count of segment j;
@@ -355,21 +364,6 @@ __device__ __noinline__ void fillSelfPool(const TeamCtx& C, int nSt, int nP, int
         for (int i = lane; i < nP; i += team) S.cellOf[i] = 0;
         teamSync(team, teamIdx);
         if (lane == 0) buildPoolLevels(C, nP, live, precision, errorWord);
-}
-
-// Bits t = 9 (dz + 1) + 3 (dy + 1) + (dx + 1) of the 27 cells around
-// cell(j) whose hash is k's bucket hash(cell(k)): the cells, in the
-// reference's query order, at which its query meets k.
-__device__ __forceinline__ unsigned bucketCells(float4 cj, float4 ck, float cell, int table) {
-    const int cx = cellCoord(cj.x, cell), cy = cellCoord(cj.y, cell), cz = cellCoord(cj.z, cell);
-    const unsigned hk = hashCell(cellCoord(ck.x, cell), cellCoord(ck.y, cell), cellCoord(ck.z, cell), table);
-    unsigned m = 0u;
-    int t = 0;
-    for (int dz = -1; dz <= 1; ++dz)
-        for (int dy = -1; dy <= 1; ++dy)
-            for (int dx = -1; dx <= 1; ++dx, ++t)
-                if (hashCell(cx + dx, cy + dy, cz + dz, table) == hk) m |= 1u << t;
-    return m;
 }
 
 // Most touching substeps have a handful of touching pairs; for those the
