@@ -168,8 +168,9 @@ def test_hook_sweep_verdicts_vs_fp64_cpu(reference):
         assert np.array_equal(held_o, held_g)
         # the mixed mode agrees with FP64 at least as often as the reference kernel
         assert agree_m >= agree_g
-    # measured: 184 of 200 (the disagreements are listed above with their
-    # FP64 margins); a regression below that fails
-    assert agree_m >= 184
+    # measured: 200 of 200 in both modes (any disagreement is listed above
+    # with its FP64 margin); a regression below that fails
+    assert agree_m == 200
+    assert agree_f == 200
     # the sweep is not degenerate: both outcomes occur
     assert 0 < held_m.sum() < 3600
